@@ -1,0 +1,231 @@
+/*
+ * tsvdx4_cuda.h -- C ABI of the B200 timeSVD++ (tsvdx4) factorizer.
+ *
+ * This is the drop-in boundary for the reference's model plugin API,
+ * `trait Regressor` (src/lib.rs:616-651), as implemented by `TxModel`
+ * (src/tx.rs:457-1116) and driven by `fit2_inner`/`fit` (src/lib.rs:881-996,
+ * 764-815). A Rust shim `TxGpuModel: Regressor` binds these symbols one to
+ * one; the binding is written out in INTEGRATION.md.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (TSVD_OK == 0). On failure the
+ *    message is available from tsvd_last_error(model) (or
+ *    tsvd_last_global_error() when no model exists yet). The reference panics
+ *    on the same conditions (unwrap/expect/assert!); the shim turns a nonzero
+ *    status back into a panic.
+ *  - Host arrays are borrowed for the duration of a call only; everything the
+ *    model keeps is copied to device memory. No torch types cross this ABI.
+ *  - The training set is a full view (ratings and residuals present). The
+ *    pr set is passed as a masked view (raw_ratings = residuals = NULL), as
+ *    the reference's MaskedDataset hides held-out targets (src/lib.rs:421-455).
+ *  - A model is owned by one host thread for mutating calls (create,
+ *    fit_epoch, set_*, destroy); const calls (predict_*, rmse, get_param) may
+ *    run concurrently from several host threads, which is what `Regressor:
+ *    Sync` requires (src/lib.rs:710-722). Const calls serialise internally.
+ */
+#ifndef TSVDX4_CUDA_H
+#define TSVDX4_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSVD_ABI_VERSION 1
+
+enum tsvd_status {
+    TSVD_OK = 0,
+    TSVD_ERR_INVALID = 1,     /* bad argument, shape or unsorted input      */
+    TSVD_ERR_UNSUPPORTED = 2, /* configuration outside the tsvdx4 path      */
+    TSVD_ERR_CUDA = 3,        /* CUDA runtime error (message has details)   */
+    TSVD_ERR_NO_DEVICE = 4,   /* no usable sm_100 device                    */
+    TSVD_ERR_OOM = 5,         /* device allocation failed                   */
+    TSVD_ERR_TIMEOUT = 6      /* a bounded device wait ran out              */
+};
+
+/* OrdinalHeadConfig (src/lib.rs:502-507). */
+typedef struct tsvd_ordinal_config {
+    float th_init[4];
+    float th_gap;
+    float lr_t;
+    float reg_t;
+} tsvd_ordinal_config;
+
+/* TxConfig (src/tx.rs:128-204), field for field and in the same order.
+ * The tsvdx4 path is tx4 mode: lr_w = lr_c = lr_w_day = lr_c_day = 0 and the
+ * w_* multipliers 1 (src/tsvdx4.rs:118-136); create() rejects a nonzero
+ * neighbourhood learning rate with TSVD_ERR_UNSUPPORTED. */
+typedef struct tsvd_config {
+    uint64_t n_feat;
+    uint64_t n_epochs;
+    uint64_t seed;
+    int32_t shuffle_users;
+    uint64_t n_time_bins;
+    float beta;
+    uint64_t n_freq_bins;
+    float lr_u, lr_ud, lr_u2, lr_ub, lr_ubd, lr_i, lr_ib, lr_y, lr_yb, lr_yd;
+    float lr_tu, lr_ti, lr_ta, lr_ibf, lr_iqf, lr_cu;
+    float reg_iqf, reg_cu, reg_u, reg_u2, reg_ud, reg_i, reg_y, reg_yd;
+    float sigma_iqf, sigma_u, sigma_i, sigma_y, sigma_yd;
+    uint64_t reset_u_epoch;
+    uint64_t max_neighbors;
+    float lr_w, lr_c, reg_w, reg_c;
+    float lr_w_day, lr_c_day, reg_w_day, reg_c_day;
+    float w_bias, w_factor, w_nbr;
+    int32_t sum_err_bug;
+    float lambda1, lambda2;
+    int32_t has_ordinal_head; /* Option<OrdinalHeadConfig>: 0 = None */
+    tsvd_ordinal_config ordinal_head;
+    int32_t save_ifeat;
+    int32_t low_memory;
+    int32_t full_su;
+} tsvd_config;
+
+/* Borrowed view of a Dataset (src/lib.rs:227-242). raw_ratings and residuals
+ * are NULL in a masked (pr) view. item_idxs is i32 as in memory (i16 on disk,
+ * widened at src/lib.rs:255-256). */
+typedef struct tsvd_dataset_view {
+    const int32_t* user_idxs;
+    const int32_t* user_cnts; /* [n_users] */
+    const int32_t* item_idxs;
+    const int32_t* item_cnts; /* [n_items], may be NULL */
+    const int8_t* raw_ratings;
+    const float* residuals;
+    const int16_t* dates;
+    const int8_t* is_test;
+    uint64_t n_users;
+    uint64_t n_items;
+    uint64_t n_ratings;
+} tsvd_dataset_view;
+
+/* Epoch schedules. */
+enum tsvd_schedule {
+    /* Users in parallel, one warp each, item-side tables updated in place as
+     * each rating is processed (the reference's per-rating update order
+     * inside a user, src/tx.rs:836-1106); concurrent users race on shared
+     * item rows. Fastest; not bitwise reproducible run to run. */
+    TSVD_SCHED_HOGWILD = 0,
+    /* Deterministic stratified schedule: the reference's own parallel
+     * schedule (src/tsvdx4p.rs:390-805): a user stratum (users in parallel,
+     * item tables frozen, NSVD1 deltas reduced in a fixed order), then an
+     * item stratum (items in parallel, user tables frozen). Bitwise
+     * reproducible for a given seed. */
+    TSVD_SCHED_STRATIFIED = 1
+};
+
+enum tsvd_precision {
+    TSVD_PREC_FP32 = 0,     /* all reads and writes FP32                     */
+    TSVD_PREC_BF16_READ = 1 /* FP32 masters; BF16 read copies of q_i and y_j */
+};
+
+/* Options that have no counterpart in TxConfig. Zero-initialised = defaults. */
+typedef struct tsvd_gpu_options {
+    int32_t schedule;        /* enum tsvd_schedule                            */
+    int32_t precision;       /* enum tsvd_precision                           */
+    float nsvd_norm_exp;     /* stratified: y-delta divisor exponent
+                                (Tsvdx4pConfig::nsvd_norm_exp), default 1.0
+                                when the whole struct is zero                  */
+    int32_t device;          /* CUDA device ordinal                           */
+    int32_t warps_per_block; /* 0 = tuned default                             */
+    int32_t reserved[8];
+} tsvd_gpu_options;
+
+typedef struct tsvd_model tsvd_model;
+
+/* ---- lifecycle -------------------------------------------------------- */
+
+/* Regressor::new / TxModel::new (src/tx.rs:460-649): computes tu_mean,
+ * day_range, SparseUD, user offsets and gbias, and draws the initial factors
+ * from StdRng(seed) in the reference's order (ufeat, ifeat, yfeat,
+ * [yfeat_day], ifeat_freq) so a seeded run starts where the reference does.
+ * opts may be NULL (defaults). */
+int tsvd_create(const tsvd_config* cfg, const tsvd_gpu_options* opts,
+                const tsvd_dataset_view* tr, const tsvd_dataset_view* pr_masked,
+                tsvd_model** out);
+void tsvd_destroy(tsvd_model* m);
+
+/* Regressor::n_epochs (src/lib.rs:626). */
+int tsvd_n_epochs(const tsvd_model* m, uint64_t* out);
+
+/* Regressor::fit_epoch (src/lib.rs:631; TxModel at src/tx.rs:734-1115).
+ * epoch is 1-based. The data were copied at create(); the reference's tr/pr
+ * arguments are therefore not passed again. */
+int tsvd_fit_epoch(tsvd_model* m, uint64_t epoch);
+
+/* ---- prediction ------------------------------------------------------- */
+
+/* Regressor::predict (src/tx.rs:713-724) for n rows at once: out[k] =
+ * predict(u[k], i[k], day[k]) in residual space. Host pointers. */
+int tsvd_predict_batch(const tsvd_model* m, const int32_t* u, const int32_t* i,
+                       const int16_t* day, uint64_t n, float* out);
+
+/* Same with device pointers, on the model's stream; no host copies. */
+int tsvd_predict_batch_device(const tsvd_model* m, const int32_t* d_u,
+                              const int32_t* d_i, const int16_t* d_day,
+                              uint64_t n, float* d_out);
+
+/* Regressor::n_subscores / subscore_names / predict_subscores
+ * (src/tx.rs:651-711): 3 columns [bias, mf, nsvd1], out is row-major [n,3]. */
+int tsvd_n_subscores(const tsvd_model* m, uint64_t* out);
+const char* tsvd_subscore_name(const tsvd_model* m, uint64_t k);
+int tsvd_predict_subscores_batch(const tsvd_model* m, const int32_t* u,
+                                 const int32_t* i, const int16_t* day,
+                                 uint64_t n, float* out);
+
+/* gen_preds_parallel (src/lib.rs:710-722): out[k] = predict(...) +
+ * (raw_ratings[k] - residuals[k]) over a full view. */
+int tsvd_gen_preds(const tsvd_model* m, const tsvd_dataset_view* ds, float* out);
+
+/* calc_rmse (src/lib.rs:659-672): FP64 sum of squared errors over the
+ * is_test == 0 rows of a full view. */
+int tsvd_calc_rmse(const tsvd_model* m, const tsvd_dataset_view* ds, double* out);
+
+/* ---- parameters ------------------------------------------------------- */
+
+/* Names: gbias, ubias, ibias, ufeat, ufeat2, ifeat, yfeat, ycache, yfeat_day,
+ * tu_mean, alpha_u, but_bin, bit_bin, ybias, ycache_bias, ubias_day,
+ * ufeat_day, ycache_day, ibias_freq, ifeat_freq, cu, cut, thresholds.
+ * All are f32, row-major, shaped as in TxModel (src/tx.rs:210-272).
+ * get copies to host; set copies from host (nbytes must match exactly).
+ * Setting yfeat/ybias does not rebuild ycache; call tsvd_rebuild_ycache. */
+int tsvd_param_nbytes(const tsvd_model* m, const char* name, uint64_t* out);
+int tsvd_get_param(const tsvd_model* m, const char* name, void* dst, uint64_t nbytes);
+int tsvd_set_param(tsvd_model* m, const char* name, const void* src, uint64_t nbytes);
+
+/* TxModel::rebuild_ycache (+ _day) (src/tx.rs:391-454). */
+int tsvd_rebuild_ycache(tsvd_model* m);
+
+/* Inject the user order of one epoch (a permutation of 0..n_users-1) in
+ * place of get_users(n, shuffle, seed, epoch) (src/lib.rs:486-494). */
+int tsvd_set_user_order(tsvd_model* m, uint64_t epoch, const uint32_t* perm, uint64_t n);
+
+/* The order get_users would produce for this epoch (rand 0.9 StdRng shuffle). */
+int tsvd_get_user_order(const tsvd_model* m, uint64_t epoch, uint32_t* perm, uint64_t n);
+
+/* ---- streams, timing, errors ------------------------------------------ */
+
+/* Launch all work of this model on `stream` (a cudaStream_t); NULL = the
+ * model's own stream. */
+int tsvd_set_stream(tsvd_model* m, void* stream);
+int tsvd_synchronize(const tsvd_model* m);
+
+/* Per-kernel CUDA-event timing, recorded on the launching stream.
+ * Enabling adds an event pair around each launch. */
+int tsvd_set_profiling(tsvd_model* m, int32_t enabled);
+int tsvd_kernel_stats(const tsvd_model* m, const char* kernel, uint64_t* launches,
+                      double* total_ms);
+int tsvd_reset_kernel_stats(tsvd_model* m);
+/* Number of kernels this model has launched since create (or the last
+ * reset_kernel_stats). */
+int tsvd_launch_count(const tsvd_model* m, uint64_t* out);
+
+const char* tsvd_last_error(const tsvd_model* m);
+const char* tsvd_last_global_error(void);
+int tsvd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TSVDX4_CUDA_H */

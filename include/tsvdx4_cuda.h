@@ -204,6 +204,13 @@ int tsvd_set_user_order(tsvd_model* m, uint64_t epoch, const uint32_t* perm, uin
 /* The order get_users would produce for this epoch (rand 0.9 StdRng shuffle). */
 int tsvd_get_user_order(const tsvd_model* m, uint64_t epoch, uint32_t* perm, uint64_t n);
 
+/* Standalone seeded streams (no model, no device needed):
+ * get_users(n, shuffle, seed, epoch) (src/lib.rs:486-494) and the first n
+ * draws of rand_array2(.., &mut StdRng::seed_from_u64(seed), sigma)
+ * (src/lib.rs:64-67). */
+int tsvd_user_order_for_seed(uint64_t n, int32_t shuffle, uint64_t seed, uint64_t epoch, uint32_t* perm);
+int tsvd_normal_stream(uint64_t seed, float sigma, uint64_t n, float* out);
+
 /* ---- streams, timing, errors ------------------------------------------ */
 
 /* Launch all work of this model on `stream` (a cudaStream_t); NULL = the

@@ -1,0 +1,173 @@
+// Internal state of a tsvd_model: device-resident dataset, precomputed
+// per-rating records, parameter tables and scratch. Shared by the ABI,
+// setup and kernel translation units. Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tsvdx4_cuda.h"
+
+namespace tsvd {
+
+// Error carrying a tsvd_status.
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define TSVD_CUDA(call)                                                                               \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            throw ::tsvd::Error(e_ == cudaErrorMemoryAllocation ? TSVD_ERR_OOM : TSVD_ERR_CUDA,       \
+                                std::string(#call) + ": " + cudaGetErrorString(e_) + " at " __FILE__ \
+                                ":" + std::to_string(__LINE__));                                      \
+    } while (0)
+
+// Owning device allocation.
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    ~DevMem() { release(); }
+    void alloc(size_t b) {
+        release();
+        if (b == 0) b = 16;
+        TSVD_CUDA(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return (T*)p; }
+};
+
+// Packed per-rating record, 16 bytes, one coalesced load per rating.
+//   key = id (20 bits: item in the user-major stream, user in the item-major
+//         stream) | time bin << 20 (6 bits) | frequency bin << 26 (6 bits)
+//   res = residual (training target), dev = dev_u(t), ud = (user, day) index
+struct __align__(16) Rec {
+    uint32_t key;
+    float res;
+    float dev;
+    uint32_t ud;
+};
+constexpr uint32_t kIdBits = 20, kIdMask = (1u << kIdBits) - 1u;
+constexpr uint32_t kMaxBins = 64;
+
+// Kernel arguments for one model (everything a kernel may touch).
+struct DeviceState {
+    // sizes
+    uint32_t n_users, n_items, F, Fs, T, NF;
+    uint64_t n_train, n_pr, n_ud;
+    int32_t day_range;
+    float gbias;
+    // dataset
+    const Rec* rec;            // [n_train] user-major, rating order
+    const uint64_t* user_off;  // [U+1]
+    const Rec* irec;           // [n_train] item-major (by-item index order)
+    const uint64_t* item_off;  // [I+1]
+    const uint32_t* pr_item;   // [n_pr] pr items grouped by user, pr order within user
+    const uint64_t* pr_off;    // [U+1]
+    const int32_t* user_cnt_tr;  // [U]
+    const int32_t* user_cnt_pr;  // [U]
+    const int8_t* raw;         // [n_train] raw ratings (ordinal head only)
+    const uint64_t* ud_start;  // [U+1]
+    const int16_t* ud_date;    // [n_ud]
+    const uint32_t* ud_cnt;    // [n_ud]
+    const float* tu_mean;      // [U]
+    // parameters (feature rows have stride Fs, zero padded)
+    float *ubias, *ibias, *ufeat, *ufeat2, *ifeat, *yfeat, *ycache, *yfeat_day;
+    float *alpha_u, *but_bin, *bit_bin, *ybias, *ycache_bias;
+    float *ubias_day, *ufeat_day, *ycache_day;
+    float *ibias_freq, *ifeat_freq, *cu, *cut;
+    float* thresholds;  // [4] ordinal head
+    // stratified scratch
+    float* g_user;   // [U, Fs] per-user NSVD1 gradient sum / norm
+    float* e_user;   // [U]     per-user error sum / norm
+    // work lists
+    const uint32_t* user_work;  // users in processing order
+    const uint32_t* item_work;  // items in processing order
+    uint32_t* counters;         // [8] dynamic work counters
+};
+
+struct KernelStat {
+    uint64_t launches = 0;
+    double total_ms = 0.0;
+};
+
+}  // namespace tsvd
+
+struct tsvd_model {
+    tsvd_config cfg{};
+    tsvd_gpu_options opts{};
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    mutable std::mutex mu;
+    mutable std::string err;
+
+    tsvd::DeviceState d{};
+    bool ycache_valid = false;  // ycache equals a rebuild from the current yfeat
+    uint64_t launches = 0;
+
+    // device allocations
+    tsvd::DevMem m_rec, m_user_off, m_irec, m_item_off, m_pr_item, m_pr_off, m_ucnt_tr, m_ucnt_pr, m_raw;
+    tsvd::DevMem m_ud_start, m_ud_date, m_ud_cnt, m_tu_mean;
+    tsvd::DevMem m_ubias, m_ibias, m_ufeat, m_ufeat2, m_ifeat, m_yfeat, m_ycache, m_yfeat_day;
+    tsvd::DevMem m_alpha_u, m_but_bin, m_bit_bin, m_ybias, m_ycache_bias;
+    tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
+    tsvd::DevMem m_g_user, m_e_user, m_user_work, m_item_work, m_counters;
+    tsvd::DevMem m_perm;          // [U] epoch order upload buffer
+    tsvd::DevMem m_scratch;       // predict / rmse scratch
+    size_t scratch_rows = 0;
+
+    std::vector<uint32_t> h_user_cnt;  // train counts (host copy)
+    std::map<uint64_t, std::vector<uint32_t>> injected_order;
+
+    // profiling
+    bool profiling = false;
+    std::map<std::string, tsvd::KernelStat> stats;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+
+namespace tsvd {
+
+// setup (tsvd_setup.cu)
+void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_view& pr);
+// epoch drivers (tsvd_epoch.cu)
+void run_epoch(tsvd_model* m, uint64_t epoch);
+void rebuild_ycache(tsvd_model* m);
+// predictions (tsvd_predict.cu)
+void predict_device(const tsvd_model* m, const int32_t* u, const int32_t* i, const int16_t* day,
+                    const float* offset, uint64_t n, float* out, int subscores);
+void sse_device(const tsvd_model* m, const int32_t* u, const int32_t* i, const int16_t* day, const float* target,
+                const int8_t* is_test, uint64_t n, double* out_sse, double* out_cnt);
+
+// profiling helpers (tsvd_abi.cu)
+void prof_begin(tsvd_model* m, const char* name, cudaEvent_t* ev_pair);
+void prof_end(tsvd_model* m, const char* name, cudaEvent_t* ev_pair);
+
+// RAII scope that records an event pair around launches when profiling.
+struct ProfScope {
+    tsvd_model* m;
+    const char* name;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ProfScope(tsvd_model* mm, const char* n) : m(mm), name(n) { prof_begin(m, name, ev); }
+    ~ProfScope() { prof_end(m, name, ev); }
+};
+
+inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace tsvd

@@ -1,0 +1,184 @@
+// Batched prediction: TxModel::predict (src/tx.rs:713-724 via factor_parts
+// :303-339), predict_subscores (:651-711), and the FP64 sum of squared errors
+// behind calc_rmse (src/lib.rs:659-672). One warp per row; the SSE is reduced
+// in a fixed order (per-warp sums, per-block tree, then one block over the
+// block partials), so repeated calls are bitwise identical.
+#include "tsvd_device.cuh"
+
+namespace tsvd {
+namespace {
+
+constexpr int kWarps = 8, kThreads = 256;
+constexpr unsigned kSseBlocks = 148 * 4;
+
+struct PredParams {
+    float beta;
+    int32_t low_memory;
+};
+
+template <int VPL>
+__device__ __forceinline__ void predict_row(const DeviceState& s, const PredParams& pp, uint32_t u, uint32_t i,
+                                            int16_t day, int lane, float& bias_part, float& dot, float* subs) {
+    const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
+    const uint32_t b = time_bin(day, s.day_range, T);
+    const float dv = dev_of(day, s.tu_mean[u], pp.beta);
+    const uint32_t idx = ud_index(s, u, day);
+    const bool has = idx != 0xffffffffu;
+    const uint32_t f = has ? freq_bin(s.ud_cnt[idx], NF) : 0u;
+    const float bu_day = has ? s.ubias_day[idx] : 0.0f;
+    const float ubu = s.ubias[u], but = s.but_bin[(size_t)u * T + b], al = s.alpha_u[u], ycb = s.ycache_bias[u];
+    const float ibi = s.ibias[i], bit = s.bit_bin[(size_t)i * T + b], ibf = s.ibias_freq[(size_t)i * NF + f];
+    const float bu_t = ubu + but + al * dv + bu_day + ycb;
+    const float bi_t = ibi + bit + ibf;
+    const float cu_t = s.cu[u] + (has ? s.cut[idx] : 0.0f);
+    float pu[VPL], p2[VPL], su[VPL], q[VPL], qf[VPL];
+    Row<VPL>::load_nc(s.ufeat + (size_t)u * Fs, lane, pu);
+    Row<VPL>::load_nc(s.ufeat2 + (size_t)u * Fs, lane, p2);
+    Row<VPL>::load_nc(s.ycache + (size_t)u * Fs, lane, su);
+    Row<VPL>::load_nc(s.ifeat + (size_t)i * Fs, lane, q);
+    Row<VPL>::load_nc(s.ifeat_freq + ((size_t)i * NF + f) * Fs, lane, qf);
+    if (subs) {
+        float mf = 0.0f, ns = 0.0f;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+            const float qe = q[v] + qf[v];
+            mf += (pu[v] + dv * p2[v]) * qe;
+            ns += su[v] * qe;
+        }
+        mf = warp_sum(mf);
+        ns = warp_sum(ns);
+        subs[0] = s.gbias + ubu + ibi + ibf + but + al * dv + bu_day + bit + bi_t * (cu_t - 1.0f) + ycb;
+        subs[1] = mf;
+        subs[2] = ns;
+    } else {
+        float part = 0.0f;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) part += ((pu[v] + su[v]) + dv * p2[v]) * (q[v] + qf[v]);
+        dot = warp_sum(part);
+        bias_part = s.gbias + bu_t + bi_t * cu_t;
+    }
+}
+
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_predict(DeviceState s, PredParams pp, const int32_t* __restrict__ u,
+                                                      const int32_t* __restrict__ it, const int16_t* __restrict__ d,
+                                                      const float* __restrict__ offset, uint64_t n,
+                                                      float* __restrict__ out, int subscores) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * kWarps;
+    for (uint64_t r = blockIdx.x * (uint64_t)kWarps + (threadIdx.x >> 5); r < n; r += warps) {
+        float bp = 0.0f, dot = 0.0f, sub[3];
+        predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, subscores ? sub : nullptr);
+        if (lane == 0) {
+            if (subscores) {
+                out[3 * r] = sub[0];
+                out[3 * r + 1] = sub[1];
+                out[3 * r + 2] = sub[2];
+            } else {
+                float score = bp + dot + 0.0f;
+                out[r] = offset ? score + offset[r] : score;
+            }
+        }
+    }
+}
+
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_sse(DeviceState s, PredParams pp, const int32_t* __restrict__ u,
+                                                  const int32_t* __restrict__ it, const int16_t* __restrict__ d,
+                                                  const float* __restrict__ target, const int8_t* __restrict__ is_test,
+                                                  uint64_t n, double* __restrict__ part_sse,
+                                                  double* __restrict__ part_cnt) {
+    __shared__ double ssh[kWarps], csh[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t warps = (uint64_t)gridDim.x * kWarps;
+    double sse = 0.0, cnt = 0.0;
+    for (uint64_t r = blockIdx.x * (uint64_t)kWarps + warp; r < n; r += warps) {
+        if (is_test && is_test[r] != 0) continue;
+        float bp = 0.0f, dot = 0.0f;
+        predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, nullptr);
+        const float e = (bp + dot + 0.0f) - target[r];
+        const double ed = (double)e;
+        sse += ed * ed;
+        cnt += 1.0;
+    }
+    if (lane == 0) {
+        ssh[warp] = sse;
+        csh[warp] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            a += ssh[w];
+            c += csh[w];
+        }
+        part_sse[blockIdx.x] = a;
+        part_cnt[blockIdx.x] = c;
+    }
+}
+
+__global__ void k_sse_final(const double* __restrict__ ps, const double* __restrict__ pc, unsigned nb,
+                            double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (unsigned b = 0; b < nb; ++b) {
+            a += ps[b];
+            c += pc[b];
+        }
+        out[0] = a;
+        out[1] = c;
+    }
+}
+
+#define TSVD_DISPATCH(VPLV, CALL)                                              \
+    switch (VPLV) {                                                            \
+        case 1: { constexpr int V = 1; CALL; } break;                          \
+        case 2: { constexpr int V = 2; CALL; } break;                          \
+        case 3: { constexpr int V = 3; CALL; } break;                          \
+        case 4: { constexpr int V = 4; CALL; } break;                          \
+        case 5: { constexpr int V = 5; CALL; } break;                          \
+        case 6: { constexpr int V = 6; CALL; } break;                          \
+        case 7: { constexpr int V = 7; CALL; } break;                          \
+        case 8: { constexpr int V = 8; CALL; } break;                          \
+        default: throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256");       \
+    }
+
+}  // namespace
+
+void predict_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, const int16_t* day, const float* offset,
+                    uint64_t n, float* out, int subscores) {
+    tsvd_model* m = const_cast<tsvd_model*>(mc);
+    if (n == 0) return;
+    ProfScope ps(m, subscores ? "predict_subscores" : "predict");
+    PredParams pp{m->cfg.beta, m->cfg.low_memory};
+    const int vpl = (int)(m->d.Fs / 32);
+    unsigned grid = (unsigned)std::min<uint64_t>((n + kWarps - 1) / kWarps, 148ull * 16);
+    TSVD_DISPATCH(vpl, (k_predict<V><<<grid, kThreads, 0, m->stream>>>(m->d, pp, u, i, day, offset, n, out, subscores)));
+    TSVD_CUDA(cudaGetLastError());
+    m->launches++;
+}
+
+void sse_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, const int16_t* day, const float* target,
+                const int8_t* is_test, uint64_t n, double* out_sse, double* out_cnt) {
+    tsvd_model* m = const_cast<tsvd_model*>(mc);
+    ProfScope ps(m, "sse");
+    PredParams pp{m->cfg.beta, m->cfg.low_memory};
+    const int vpl = (int)(m->d.Fs / 32);
+    DevMem part;
+    part.alloc((2 * kSseBlocks + 2) * sizeof(double));
+    double* psse = part.as<double>();
+    double* pcnt = psse + kSseBlocks;
+    double* fin = pcnt + kSseBlocks;
+    TSVD_DISPATCH(vpl, (k_sse<V><<<kSseBlocks, kThreads, 0, m->stream>>>(m->d, pp, u, i, day, target, is_test, n, psse,
+                                                                         pcnt)));
+    k_sse_final<<<1, 32, 0, m->stream>>>(psse, pcnt, kSseBlocks, fin);
+    TSVD_CUDA(cudaGetLastError());
+    m->launches += 2;
+    double h[2];
+    TSVD_CUDA(cudaMemcpyAsync(h, fin, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+    TSVD_CUDA(cudaStreamSynchronize(m->stream));
+    *out_sse = h[0];
+    *out_cnt = h[1];
+}
+
+}  // namespace tsvd

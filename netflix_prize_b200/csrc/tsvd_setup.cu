@@ -1,0 +1,389 @@
+// Model construction: the device-side counterpart of TxModel::new
+// (src/tx.rs:460-649) plus the one-time per-rating precompute that the
+// reference repeats inside every epoch (time_bin, dev and the SparseUD
+// binary search at src/tx.rs:841-842,878; freq_bin at :851).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "rand_stream.hpp"
+#include "tsvd_device.cuh"
+
+namespace tsvd {
+namespace {
+
+__global__ void k_ud_keys(const int32_t* __restrict__ u, const int16_t* __restrict__ d, uint64_t n,
+                          uint64_t* __restrict__ keys) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x)
+        keys[t] = ((uint64_t)(uint32_t)u[t] << 16) | (uint64_t)(uint16_t)((int32_t)d[t] + 32768);
+}
+
+__global__ void k_ud_split(const uint64_t* __restrict__ ukeys, const uint32_t* __restrict__ cnts, uint64_t n_ud,
+                           int16_t* __restrict__ date, uint32_t* __restrict__ cnt_out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_ud; k += (uint64_t)gridDim.x * blockDim.x) {
+        date[k] = (int16_t)((int32_t)(ukeys[k] & 0xffff) - 32768);
+        cnt_out[k] = cnts[k];
+    }
+}
+
+// start[u] = first k with user(key[k]) >= u, for u in [0, U].
+__global__ void k_lower_bound_users(const uint64_t* __restrict__ ukeys, uint64_t n, uint32_t U,
+                                    uint64_t* __restrict__ start) {
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u <= U; u += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t lo = 0, hi = n, target = u << 16;
+        while (lo < hi) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (ukeys[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        start[u] = lo;
+    }
+}
+
+__global__ void k_records(DeviceState s, const int32_t* __restrict__ u, const int32_t* __restrict__ it,
+                          const int16_t* __restrict__ d, const float* __restrict__ res, float beta,
+                          Rec* __restrict__ out) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < s.n_train;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t uu = (uint32_t)u[t];
+        int16_t day = d[t];
+        uint32_t tb = time_bin(day, s.day_range, s.T);
+        uint32_t ud = ud_index(s, uu, day);
+        uint32_t fb = ud == 0xffffffffu ? 0u : freq_bin(s.ud_cnt[ud], s.NF);
+        Rec r;
+        r.key = ((uint32_t)it[t] & kIdMask) | (tb << 20) | (fb << 26);
+        r.res = res[t];
+        r.dev = dev_of(day, s.tu_mean[uu], beta);
+        r.ud = ud;
+        out[t] = r;
+    }
+}
+
+__global__ void k_item_records(const Rec* __restrict__ rec, const int32_t* __restrict__ u,
+                               const uint32_t* __restrict__ order, uint64_t n, Rec* __restrict__ out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t t = order[k];
+        Rec r = rec[t];
+        r.key = ((uint32_t)u[t] & kIdMask) | (r.key & ~kIdMask);
+        out[k] = r;
+    }
+}
+
+__global__ void k_gather_u32(const int32_t* __restrict__ src, const uint32_t* __restrict__ idx, uint64_t n,
+                             uint32_t* __restrict__ out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        out[k] = (uint32_t)src[idx[k]];
+}
+
+__global__ void k_iota(uint32_t* __restrict__ v, uint64_t n) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        v[k] = (uint32_t)k;
+}
+
+__global__ void k_fill(float* __restrict__ v, uint64_t n, float x) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        v[k] = x;
+}
+
+constexpr unsigned kGrid = 148 * 8, kBlock = 256;
+
+template <class T>
+void upload(DevMem& m, const T* src, size_t n, cudaStream_t st) {
+    m.alloc(n * sizeof(T));
+    if (n) TSVD_CUDA(cudaMemcpyAsync(m.p, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+void zeros(DevMem& m, size_t bytes, cudaStream_t st) {
+    m.alloc(bytes);
+    TSVD_CUDA(cudaMemsetAsync(m.p, 0, m.bytes, st));
+}
+
+// Stable radix sort of (key, value) pairs over the low `bits` key bits.
+template <class K>
+void sort_pairs(DevMem& tmp, const K* kin, K* kout, const uint32_t* vin, uint32_t* vout, uint64_t n, int bits,
+                cudaStream_t st) {
+    size_t need = 0;
+    TSVD_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need, kin, kout, vin, vout, (int64_t)n, 0, bits, st));
+    if (tmp.bytes < need) tmp.alloc(need);
+    size_t have = tmp.bytes;
+    TSVD_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, have, kin, kout, vin, vout, (int64_t)n, 0, bits, st));
+}
+
+int bits_for(uint64_t maxv) {
+    int b = 1;
+    while (b < 64 && (maxv >> b) != 0) ++b;
+    return b;
+}
+
+}  // namespace
+
+void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_view& pr) {
+    const tsvd_config& c = m->cfg;
+    cudaStream_t st = m->stream;
+    DeviceState& s = m->d;
+    // ---- validation (the reference panics on the same conditions) ----------
+    if (!tr.user_idxs || !tr.item_idxs || !tr.residuals || !tr.dates || !tr.user_cnts)
+        throw Error(TSVD_ERR_INVALID, "training view lacks user_idxs/item_idxs/residuals/dates/user_cnts");
+    if (!pr.user_idxs || !pr.item_idxs || !pr.dates || !pr.user_cnts)
+        throw Error(TSVD_ERR_INVALID, "pr view lacks user_idxs/item_idxs/dates/user_cnts");
+    if (pr.n_users != tr.n_users) throw Error(TSVD_ERR_INVALID, "train and pr disagree on n_users");
+    if (c.lr_w != 0 || c.lr_c != 0 || c.lr_w_day != 0 || c.lr_c_day != 0)
+        throw Error(TSVD_ERR_UNSUPPORTED, "neighbourhood terms (tx5/tx6) are outside the tsvdx4 path");
+    if (c.n_feat < 1 || c.n_feat > 256) throw Error(TSVD_ERR_UNSUPPORTED, "n_feat must be in 1..256");
+    if (c.n_time_bins < 1 || c.n_time_bins > kMaxBins) throw Error(TSVD_ERR_UNSUPPORTED, "n_time_bins must be in 1..64");
+    if (c.n_freq_bins < 1 || c.n_freq_bins > kMaxBins) throw Error(TSVD_ERR_UNSUPPORTED, "n_freq_bins must be in 1..64");
+    if (tr.n_users == 0 || tr.n_users > (1u << kIdBits) || tr.n_items == 0 || tr.n_items > (1u << kIdBits))
+        throw Error(TSVD_ERR_UNSUPPORTED, "n_users and n_items must be in 1..2^20");
+    if (tr.n_ratings == 0) throw Error(TSVD_ERR_INVALID, "empty training set");
+    if (tr.n_ratings >= (1ull << 32) || pr.n_ratings >= (1ull << 32))
+        throw Error(TSVD_ERR_UNSUPPORTED, "at most 2^32-1 ratings per set");
+    if (!c.low_memory) throw Error(TSVD_ERR_UNSUPPORTED, "low_memory = false (per-day NSVD1 terms) is not built yet");
+    if (c.has_ordinal_head) throw Error(TSVD_ERR_UNSUPPORTED, "the ordinal head is not built yet");
+
+    const uint32_t U = (uint32_t)tr.n_users, I = (uint32_t)tr.n_items;
+    const uint64_t R = tr.n_ratings, P = pr.n_ratings;
+    // calc_user_offsets (src/lib.rs:470-483): user-sorted, offsets from user_cnts.
+    std::vector<uint64_t> uoff(U + 1, 0);
+    for (uint32_t u = 0; u < U; ++u) {
+        if (tr.user_cnts[u] < 0) throw Error(TSVD_ERR_INVALID, "negative user count");
+        uoff[u + 1] = uoff[u] + (uint64_t)tr.user_cnts[u];
+    }
+    if (uoff[U] != R) throw Error(TSVD_ERR_INVALID, "training user_cnts do not sum to n_ratings");
+    {
+        uint32_t prev = 0;
+        for (uint64_t t = 0; t < R; ++t) {
+            int32_t u = tr.user_idxs[t];
+            if (u < 0 || (uint32_t)u >= U) throw Error(TSVD_ERR_INVALID, "training user index out of range");
+            if ((uint32_t)u < prev)
+                throw Error(TSVD_ERR_INVALID, "training set is not user-sorted at index " + std::to_string(t));
+            prev = (uint32_t)u;
+            int32_t i = tr.item_idxs[t];
+            if (i < 0 || (uint32_t)i >= I) throw Error(TSVD_ERR_INVALID, "training item index out of range");
+        }
+        for (uint32_t u = 0; u < U; ++u) {
+            uint64_t e = uoff[u + 1];
+            if (e > uoff[u] && ((uint32_t)tr.user_idxs[uoff[u]] != u || (uint32_t)tr.user_idxs[e - 1] != u))
+                throw Error(TSVD_ERR_INVALID, "training user_cnts disagree with user_idxs");
+        }
+        std::vector<int64_t> pcnt(U, 0);
+        for (uint64_t t = 0; t < P; ++t) {
+            int32_t u = pr.user_idxs[t], i = pr.item_idxs[t];
+            if (u < 0 || (uint32_t)u >= U || i < 0 || (uint32_t)i >= I)
+                throw Error(TSVD_ERR_INVALID, "pr index out of range");
+            pcnt[u]++;
+        }
+        for (uint32_t u = 0; u < U; ++u)
+            if (pcnt[u] != pr.user_cnts[u]) throw Error(TSVD_ERR_INVALID, "pr user_cnts disagree with user_idxs");
+    }
+    // tu_mean in f32, summed in rating order; day_range; gbias (src/tx.rs:465-475, src/lib.rs:463-467)
+    std::vector<float> tum(U, 0.0f);
+    int32_t dr = 0;
+    double rsum = 0.0;
+    for (uint64_t t = 0; t < R; ++t) {
+        tum[tr.user_idxs[t]] += (float)tr.dates[t];
+        dr = std::max(dr, (int32_t)tr.dates[t] + 1);
+        rsum += (double)tr.residuals[t];
+    }
+    for (uint32_t u = 0; u < U; ++u)
+        if (tr.user_cnts[u] > 0) tum[u] /= (float)tr.user_cnts[u];
+    if (dr <= 0) throw Error(TSVD_ERR_INVALID, "training dates must include a non-negative day");
+
+    const uint32_t F = (uint32_t)c.n_feat;
+    const uint32_t Fs = (F + 31) / 32 * 32;
+    s.n_users = U; s.n_items = I; s.F = F; s.Fs = Fs;
+    s.T = (uint32_t)c.n_time_bins; s.NF = (uint32_t)c.n_freq_bins;
+    s.n_train = R; s.n_pr = P;
+    s.day_range = dr;
+    s.gbias = (float)(rsum / (double)R);
+    m->h_user_cnt.assign(tr.user_cnts, tr.user_cnts + U);
+
+    // ---- upload raw columns -------------------------------------------------
+    DevMem d_tu, d_ti, d_td, d_tres, d_pu, d_pi, d_pd, tmp;
+    upload(d_tu, tr.user_idxs, R, st);
+    upload(d_ti, tr.item_idxs, R, st);
+    upload(d_td, tr.dates, R, st);
+    upload(d_tres, tr.residuals, R, st);
+    upload(d_pu, pr.user_idxs, P, st);
+    upload(d_pi, pr.item_idxs, P, st);
+    upload(d_pd, pr.dates, P, st);
+    upload(m->m_user_off, uoff.data(), U + 1, st);
+    upload(m->m_tu_mean, tum.data(), U, st);
+    upload(m->m_ucnt_tr, tr.user_cnts, U, st);
+    upload(m->m_ucnt_pr, pr.user_cnts, U, st);
+    s.user_off = m->m_user_off.as<uint64_t>();
+    s.tu_mean = m->m_tu_mean.as<float>();
+    s.user_cnt_tr = m->m_ucnt_tr.as<int32_t>();
+    s.user_cnt_pr = m->m_ucnt_pr.as<int32_t>();
+
+    // ---- SparseUD over train + pr (src/tx.rs:21-84) -------------------------
+    {
+        DevMem keys, keys_sorted, ukeys, ucnt, nrun;
+        keys.alloc((R + P) * 8);
+        keys_sorted.alloc((R + P) * 8);
+        k_ud_keys<<<kGrid, kBlock, 0, st>>>(d_tu.as<int32_t>(), d_td.as<int16_t>(), R, keys.as<uint64_t>());
+        if (P) k_ud_keys<<<kGrid, kBlock, 0, st>>>(d_pu.as<int32_t>(), d_pd.as<int16_t>(), P, keys.as<uint64_t>() + R);
+        TSVD_CUDA(cudaGetLastError());
+        int kb = 16 + bits_for(U);
+        size_t need = 0;
+        TSVD_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, need, keys.as<uint64_t>(), keys_sorted.as<uint64_t>(),
+                                                 (int64_t)(R + P), 0, kb, st));
+        tmp.alloc(need);
+        size_t have = tmp.bytes;
+        TSVD_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, have, keys.as<uint64_t>(), keys_sorted.as<uint64_t>(),
+                                                 (int64_t)(R + P), 0, kb, st));
+        ukeys.alloc((R + P) * 8);
+        ucnt.alloc((R + P) * 4);
+        nrun.alloc(8);
+        need = 0;
+        TSVD_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, need, keys_sorted.as<uint64_t>(), ukeys.as<uint64_t>(),
+                                                     ucnt.as<uint32_t>(), nrun.as<int64_t>(), (int64_t)(R + P), st));
+        if (tmp.bytes < need) tmp.alloc(need);
+        have = tmp.bytes;
+        TSVD_CUDA(cub::DeviceRunLengthEncode::Encode(tmp.p, have, keys_sorted.as<uint64_t>(), ukeys.as<uint64_t>(),
+                                                     ucnt.as<uint32_t>(), nrun.as<int64_t>(), (int64_t)(R + P), st));
+        int64_t n_ud = 0;
+        TSVD_CUDA(cudaMemcpyAsync(&n_ud, nrun.p, 8, cudaMemcpyDeviceToHost, st));
+        TSVD_CUDA(cudaStreamSynchronize(st));
+        s.n_ud = (uint64_t)n_ud;
+        m->m_ud_date.alloc(n_ud * 2);
+        m->m_ud_cnt.alloc(n_ud * 4);
+        m->m_ud_start.alloc((U + 1) * 8);
+        k_ud_split<<<kGrid, kBlock, 0, st>>>(ukeys.as<uint64_t>(), ucnt.as<uint32_t>(), n_ud, m->m_ud_date.as<int16_t>(),
+                                             m->m_ud_cnt.as<uint32_t>());
+        k_lower_bound_users<<<ceil_div(U + 1, kBlock), kBlock, 0, st>>>(ukeys.as<uint64_t>(), n_ud, U,
+                                                                       m->m_ud_start.as<uint64_t>());
+        TSVD_CUDA(cudaGetLastError());
+        s.ud_start = m->m_ud_start.as<uint64_t>();
+        s.ud_date = m->m_ud_date.as<int16_t>();
+        s.ud_cnt = m->m_ud_cnt.as<uint32_t>();
+        TSVD_CUDA(cudaStreamSynchronize(st));
+    }
+
+    // ---- per-rating records (user-major) -------------------------------------
+    m->m_rec.alloc(R * sizeof(Rec));
+    k_records<<<kGrid, kBlock, 0, st>>>(s, d_tu.as<int32_t>(), d_ti.as<int32_t>(), d_td.as<int16_t>(),
+                                        d_tres.as<float>(), c.beta, m->m_rec.as<Rec>());
+    TSVD_CUDA(cudaGetLastError());
+    s.rec = m->m_rec.as<Rec>();
+
+    // ---- pr items grouped by user, pr order kept (probe_items_by_user) ------
+    {
+        DevMem idx, idx_sorted, ukey, ukey_sorted;
+        m->m_pr_item.alloc(P * 4);
+        if (P) {
+            idx.alloc(P * 4);
+            idx_sorted.alloc(P * 4);
+            ukey.alloc(P * 4);
+            ukey_sorted.alloc(P * 4);
+            k_iota<<<kGrid, kBlock, 0, st>>>(idx.as<uint32_t>(), P);
+            TSVD_CUDA(cudaMemcpyAsync(ukey.p, d_pu.p, P * 4, cudaMemcpyDeviceToDevice, st));
+            sort_pairs(tmp, ukey.as<uint32_t>(), ukey_sorted.as<uint32_t>(), idx.as<uint32_t>(),
+                       idx_sorted.as<uint32_t>(), P, bits_for(U), st);
+            k_gather_u32<<<kGrid, kBlock, 0, st>>>(d_pi.as<int32_t>(), idx_sorted.as<uint32_t>(), P,
+                                                   m->m_pr_item.as<uint32_t>());
+            TSVD_CUDA(cudaGetLastError());
+        }
+        std::vector<uint64_t> poff(U + 1, 0);
+        for (uint32_t u = 0; u < U; ++u) poff[u + 1] = poff[u] + (uint64_t)pr.user_cnts[u];
+        upload(m->m_pr_off, poff.data(), U + 1, st);
+        s.pr_item = m->m_pr_item.as<uint32_t>();
+        s.pr_off = m->m_pr_off.as<uint64_t>();
+        TSVD_CUDA(cudaStreamSynchronize(st));
+    }
+
+    // ---- by-item index (ByItemIndex, src/tsvdx4p.rs:29-57) -------------------
+    {
+        DevMem idx, idx_sorted, ikey, ikey_sorted;
+        idx.alloc(R * 4);
+        idx_sorted.alloc(R * 4);
+        ikey.alloc(R * 4);
+        ikey_sorted.alloc(R * 4);
+        k_iota<<<kGrid, kBlock, 0, st>>>(idx.as<uint32_t>(), R);
+        TSVD_CUDA(cudaMemcpyAsync(ikey.p, d_ti.p, R * 4, cudaMemcpyDeviceToDevice, st));
+        sort_pairs(tmp, ikey.as<uint32_t>(), ikey_sorted.as<uint32_t>(), idx.as<uint32_t>(), idx_sorted.as<uint32_t>(),
+                   R, bits_for(I), st);
+        m->m_irec.alloc(R * sizeof(Rec));
+        k_item_records<<<kGrid, kBlock, 0, st>>>(m->m_rec.as<Rec>(), d_tu.as<int32_t>(), idx_sorted.as<uint32_t>(), R,
+                                                 m->m_irec.as<Rec>());
+        TSVD_CUDA(cudaGetLastError());
+        std::vector<uint64_t> ioff(I + 1, 0);
+        std::vector<uint32_t> icnt(I, 0);
+        for (uint64_t t = 0; t < R; ++t) icnt[tr.item_idxs[t]]++;
+        for (uint32_t i = 0; i < I; ++i) ioff[i + 1] = ioff[i] + icnt[i];
+        upload(m->m_item_off, ioff.data(), I + 1, st);
+        s.irec = m->m_irec.as<Rec>();
+        s.item_off = m->m_item_off.as<uint64_t>();
+        // work lists: heaviest first (longest-processing-time order)
+        std::vector<uint32_t> iw(I);
+        std::iota(iw.begin(), iw.end(), 0u);
+        std::stable_sort(iw.begin(), iw.end(), [&](uint32_t a, uint32_t b) { return icnt[a] > icnt[b]; });
+        upload(m->m_item_work, iw.data(), I, st);
+        std::vector<uint32_t> uw(U);
+        std::iota(uw.begin(), uw.end(), 0u);
+        std::stable_sort(uw.begin(), uw.end(),
+                         [&](uint32_t a, uint32_t b) { return tr.user_cnts[a] > tr.user_cnts[b]; });
+        upload(m->m_user_work, uw.data(), U, st);
+        s.item_work = m->m_item_work.as<uint32_t>();
+        s.user_work = m->m_user_work.as<uint32_t>();
+        TSVD_CUDA(cudaStreamSynchronize(st));
+    }
+
+    // ---- parameters (TxModel::new field order, src/tx.rs:600-648) -----------
+    {
+        const size_t NF = c.n_freq_bins, T = c.n_time_bins;
+        ChaCha12Stream g(c.seed);
+        std::vector<float> h;
+        auto normal_table = [&](DevMem& dst, size_t rows, float sigma) {
+            h.assign(rows * Fs, 0.0f);
+            fill_normal_rows(g, sigma, rows, F, h.data(), Fs);
+            upload(dst, h.data(), h.size(), st);
+            TSVD_CUDA(cudaStreamSynchronize(st));  // h is reused
+        };
+        normal_table(m->m_ufeat, U, c.sigma_u);
+        zeros(m->m_ufeat2, (size_t)U * Fs * 4, st);
+        normal_table(m->m_ifeat, I, c.sigma_i);
+        normal_table(m->m_yfeat, I, c.sigma_y);
+        zeros(m->m_ycache, (size_t)U * Fs * 4, st);
+        // yfeat_day would be drawn here when !low_memory
+        zeros(m->m_alpha_u, U * 4, st);
+        zeros(m->m_but_bin, (size_t)U * T * 4, st);
+        zeros(m->m_bit_bin, (size_t)I * T * 4, st);
+        zeros(m->m_ybias, I * 4, st);
+        zeros(m->m_ycache_bias, U * 4, st);
+        zeros(m->m_ubias_day, s.n_ud * 4, st);
+        zeros(m->m_ibias_freq, (size_t)I * NF * 4, st);
+        normal_table(m->m_ifeat_freq, (size_t)I * NF, c.sigma_iqf);
+        zeros(m->m_ubias, U * 4, st);
+        zeros(m->m_ibias, I * 4, st);
+        m->m_cu.alloc(U * 4);
+        k_fill<<<kGrid, kBlock, 0, st>>>(m->m_cu.as<float>(), U, 1.0f);
+        TSVD_CUDA(cudaGetLastError());
+        zeros(m->m_cut, s.n_ud * 4, st);
+        zeros(m->m_thresholds, 16, st);
+        zeros(m->m_g_user, (size_t)U * Fs * 4, st);
+        zeros(m->m_e_user, U * 4, st);
+        zeros(m->m_counters, 64, st);
+        m->m_perm.alloc(U * 4);
+        s.ubias = m->m_ubias.as<float>(); s.ibias = m->m_ibias.as<float>();
+        s.ufeat = m->m_ufeat.as<float>(); s.ufeat2 = m->m_ufeat2.as<float>();
+        s.ifeat = m->m_ifeat.as<float>(); s.yfeat = m->m_yfeat.as<float>();
+        s.ycache = m->m_ycache.as<float>(); s.yfeat_day = nullptr;
+        s.alpha_u = m->m_alpha_u.as<float>(); s.but_bin = m->m_but_bin.as<float>();
+        s.bit_bin = m->m_bit_bin.as<float>(); s.ybias = m->m_ybias.as<float>();
+        s.ycache_bias = m->m_ycache_bias.as<float>(); s.ubias_day = m->m_ubias_day.as<float>();
+        s.ufeat_day = nullptr; s.ycache_day = nullptr;
+        s.ibias_freq = m->m_ibias_freq.as<float>(); s.ifeat_freq = m->m_ifeat_freq.as<float>();
+        s.cu = m->m_cu.as<float>(); s.cut = m->m_cut.as<float>();
+        s.thresholds = m->m_thresholds.as<float>();
+        s.g_user = m->m_g_user.as<float>(); s.e_user = m->m_e_user.as<float>();
+        s.counters = m->m_counters.as<uint32_t>();
+        s.raw = nullptr;
+    }
+    TSVD_CUDA(cudaStreamSynchronize(st));
+    m->ycache_valid = false;  // ycache starts at zero, as in the reference
+}
+
+}  // namespace tsvd

@@ -83,68 +83,107 @@ def _exact_total(rng, w: np.ndarray, total: int, lo: np.ndarray, hi: np.ndarray)
     raise ValueError("total not reached")
 
 
-def _sample_items(rng, cnt: np.ndarray, cdf: np.ndarray, n_items: int, exclude=None, chunk_draws=1 << 24):
-    """Per user, `cnt[u]` distinct items drawn by weight without replacement
-    (draw with replacement, keep first occurrences in draw order, top up any
-    shortfall). Keys in sorted `exclude` (user * n_items + item) are never
-    chosen. Returns (users, items) grouped by user, items in draw order."""
-    n_users = len(cnt)
+def _argsort(key: np.ndarray) -> np.ndarray:
+    """Stable argsort (identical result on every backend)."""
+    try:
+        import torch
+        if torch.cuda.is_available() and len(key) > (1 << 22):
+            t = torch.from_numpy(np.ascontiguousarray(key)).cuda()
+            return torch.sort(t, stable=True).indices.cpu().numpy()
+    except ImportError:
+        pass
+    return np.argsort(key, kind="stable")
+
+
+def _saturated_counts(n: np.ndarray, w_rank: np.ndarray) -> np.ndarray:
+    """Per user with n picks, the number m of most popular items whose
+    inclusion probability min(1, c w_k) saturates, where c solves
+    sum_k min(1, c w_k) = n (conditional Poisson sampling)."""
+    tail = np.concatenate([np.cumsum(w_rank[::-1])[::-1], [0.0]])  # tail[m] = sum_{k >= m} w_k
+    lo = np.zeros(len(n), np.int64)
+    hi = n.astype(np.int64).copy()
+    # smallest m in [0, n] with (n - m) w[m] < tail[m]
+    for _ in range(40):
+        mid = (lo + hi) // 2
+        wm = w_rank[np.minimum(mid, len(w_rank) - 1)]
+        ok = (n - mid) * wm < tail[mid]
+        hi = np.where(ok, mid, hi)
+        lo = np.where(ok, lo, mid + 1)
+        if np.all(lo >= hi):
+            break
+    return hi
+
+
+def _sample_items(rng, cnt: np.ndarray, w_rank: np.ndarray, rank_item: np.ndarray, exclude=None,
+                  chunk_draws=1 << 24):
+    """Per user, `cnt[u]` distinct items drawn without replacement with
+    popularity weights: the saturated head (see _saturated_counts) is taken
+    outright and the rest is drawn from the remaining tail by weight, each
+    round drawing exactly the users' shortfall and dropping repeats. Keys in
+    sorted `exclude` (user * n_items + item) are never chosen. Returns
+    (users, items), sorted by (user, item)."""
+    n_users, n_items = len(cnt), len(w_rank)
+    cnt = cnt.astype(np.int64)
     ex_key = exclude if exclude is not None else np.zeros(0, np.int64)
-    out_u, out_i = [], []
-    # user chunks of about chunk_draws draws each
-    per = np.ceil(cnt * 1.3).astype(np.int64) + 4
-    bounds = [0]
-    acc = 0
-    for u in range(n_users):
-        acc += int(per[u])
-        if acc >= chunk_draws:
-            bounds.append(u + 1)
-            acc = 0
-    if bounds[-1] != n_users:
-        bounds.append(n_users)
+    cdf = np.cumsum(w_rank)
+    cdf /= cdf[-1]
+    m = np.zeros(n_users, np.int64) if exclude is not None else _saturated_counts(cnt, w_rank)
+    out = []
+    csum = np.cumsum(cnt + 1)
+    bounds = [0] + list(np.searchsorted(csum, np.arange(chunk_draws, csum[-1], chunk_draws)) + 1) + [n_users]
+    bounds = sorted(set(min(int(b), n_users) for b in bounds))
     for u0, u1 in zip(bounds[:-1], bounds[1:]):
-        need = cnt[u0:u1].astype(np.int64)
-        have_k = np.zeros(0, np.int64)   # user * n_items + item
-        have_o = np.zeros(0, np.int64)   # draw order
-        order_base = 0
-        lo = np.searchsorted(ex_key, u0 * n_items)
-        hi = np.searchsorted(ex_key, u1 * n_items)
-        exk = ex_key[lo:hi]
-        for _ in range(200):
-            got = np.bincount(have_k // n_items - u0, minlength=u1 - u0) if len(have_k) else np.zeros(u1 - u0, np.int64)
-            deficit = need - got
+        if u0 == u1:
+            continue
+        users = np.arange(u0, u1, dtype=np.int64)
+        hm = m[u0:u1]
+        need = cnt[u0:u1] - hm
+        hu = np.repeat(users, hm)
+        hr = np.arange(hu.size, dtype=np.int64) - np.repeat(np.cumsum(hm) - hm, hm)
+        head_k = np.sort(hu * n_items + rank_item[hr])
+        lo_cdf = np.where(hm > 0, cdf[np.maximum(hm - 1, 0)], 0.0)
+        exk = ex_key[np.searchsorted(ex_key, u0 * n_items):np.searchsorted(ex_key, u1 * n_items)]
+        have = np.zeros(0, np.int64)  # sorted keys
+        deficit = need.copy()
+        for _ in range(60):
             if deficit.max(initial=0) <= 0:
                 break
-            draws = np.where(deficit > 0, np.ceil(deficit * 1.3).astype(np.int64) + 4, 0)
-            du = np.repeat(np.arange(u0, u1, dtype=np.int64), draws)
-            di = np.searchsorted(cdf, rng.random(len(du)), side="right").astype(np.int64)
-            np.minimum(di, n_items - 1, out=di)
-            dk = du * n_items + di
-            do = order_base + np.arange(len(dk), dtype=np.int64)
-            order_base += len(dk)
-            if len(exk):
-                pos = np.minimum(np.searchsorted(exk, dk), len(exk) - 1)
-                keep = exk[pos] != dk
-                dk, do = dk[keep], do[keep]
-            ak = np.concatenate([have_k, dk])
-            ao = np.concatenate([have_o, do])
-            s = np.argsort(ak, kind="stable")      # equal keys keep draw order
-            ak, ao = ak[s], ao[s]
-            first = np.ones(len(ak), bool)
+            du = np.repeat(users, np.maximum(deficit, 0))
+            base = lo_cdf[du - u0]
+            r = base + rng.random(du.size) * (1.0 - base)
+            rank = np.minimum(np.searchsorted(cdf, r, side="right"), n_items - 1)
+            dk = du * n_items + rank_item[rank]
+            if exk.size:
+                pos = np.minimum(np.searchsorted(exk, dk), exk.size - 1)
+                dk = dk[exk[pos] != dk]
+            ak = np.concatenate([have, dk])
+            ak = ak[_argsort(ak)]
+            first = np.ones(ak.size, bool)
             first[1:] = ak[1:] != ak[:-1]
-            ak, ao = ak[first], ao[first]
-            au = ak // n_items
-            s = np.argsort(au * order_base + ao)   # by user, then draw order
-            ak, ao, au = ak[s], ao[s], au[s]
-            starts = np.searchsorted(au, np.arange(u0, u1))
-            rank = np.arange(len(au)) - starts[au - u0]
-            keep = rank < need[au - u0]
-            have_k, have_o = ak[keep], ao[keep]
-        else:
-            raise RuntimeError("item sampling did not converge")
-        out_u.append(have_k // n_items)
-        out_i.append(have_k % n_items)
-    return np.concatenate(out_u), np.concatenate(out_i)
+            have = ak[first]
+            deficit = need - np.bincount(have // n_items - u0, minlength=u1 - u0)
+        if deficit.max(initial=0) > 0:
+            # rare: fill the remainder uniformly from the items still free
+            extra = []
+            hs = np.searchsorted(have, users * n_items)
+            he = np.searchsorted(have, (users + 1) * n_items)
+            xs = np.searchsorted(exk, users * n_items)
+            xe = np.searchsorted(exk, (users + 1) * n_items)
+            ks = np.searchsorted(head_k, users * n_items)
+            ke = np.searchsorted(head_k, (users + 1) * n_items)
+            for j in np.nonzero(deficit > 0)[0]:
+                uu = u0 + j
+                taken = np.zeros(n_items, bool)
+                taken[have[hs[j]:he[j]] % n_items] = True
+                taken[exk[xs[j]:xe[j]] % n_items] = True
+                taken[head_k[ks[j]:ke[j]] % n_items] = True
+                free = np.nonzero(~taken)[0]
+                pick = rng.choice(free, size=int(min(deficit[j], free.size)), replace=False)
+                extra.append(uu * n_items + pick)
+            have = np.concatenate([have] + extra)
+        out.append(np.sort(np.concatenate([head_k, have])))
+    allk = np.concatenate(out)
+    return allk // n_items, allk % n_items
 
 
 def generate(spec: SynthSpec):
@@ -169,11 +208,10 @@ def generate(spec: SynthSpec):
     n_rated = n_tr + n_ho
     # --- item popularity ---------------------------------------------------
     pop_rank = rng.permutation(I)            # item id -> popularity rank
+    rank_item = np.argsort(pop_rank)         # popularity rank -> item id
     w_rank = 1.0 / np.arange(1, I + 1, dtype=np.float64) ** spec.zipf_s
     w_item = w_rank[pop_rank]
-    cdf = np.cumsum(w_item)
-    cdf /= cdf[-1]
-    ru, ri = _sample_items(rng, n_rated, cdf, I)
+    ru, ri = _sample_items(rng, n_rated, w_rank, rank_item)
     # --- dates: sessions inside a personal window --------------------------
     start = rng.integers(0, N_DAYS - 1, U)
     span = np.minimum(N_DAYS - 1 - start, (rng.exponential(500.0, U) + 1).astype(np.int64))
@@ -202,28 +240,29 @@ def generate(spec: SynthSpec):
         score[a:b] = s
     rating = np.clip(np.rint(score), 1, 5).astype(np.int8)
     # --- split: each user's latest-dated n_ho ratings are held out -----------
-    tie = rng.random(len(ru))
-    o = np.lexsort((tie, rd, ru))
+    tie = rng.integers(0, 1 << 16, len(ru), dtype=np.int64)
+    o = _argsort((ru.astype(np.int64) << 32) | (rd.astype(np.int64) << 16) | tie)
     ru, ri, rd, rating = ru[o], ri[o], rd[o], rating[o]
     ustart = np.concatenate([[0], np.cumsum(n_rated)])
     pos = np.arange(len(ru)) - ustart[ru]
     held = pos >= n_tr[ru]
     # --- query pairs: unrated items, dated after the user's last rating ----
     ex = np.sort(ru.astype(np.int64) * I + ri)
-    qu, qi = _sample_items(rng, n_q, cdf, I, exclude=ex)
+    n_q = np.minimum(n_q, (I - n_rated) // 4)
+    qu, qi = _sample_items(rng, n_q, w_rank, rank_item, exclude=ex)
     last = np.zeros(U, np.int64)
     np.maximum.at(last, ru, rd)
     qd = np.minimum(N_DAYS - 1, last[qu] + rng.integers(0, 60, len(qu)))
     # --- assemble ------------------------------------------------------------
     tu, ti, td, tr_r = ru[~held], ri[~held], rd[~held], rating[~held]
-    o = np.lexsort((ti, tu))
+    o = _argsort(tu.astype(np.int64) * I + ti)
     tu, ti, td, tr_r = tu[o], ti[o], td[o], tr_r[o]
     pu = np.concatenate([ru[held], qu])
     pi = np.concatenate([ri[held], qi])
     pd_ = np.concatenate([rd[held], qd])
     pr_r = np.concatenate([rating[held], np.zeros(len(qu), np.int8)])
     pt = np.concatenate([np.zeros(int(held.sum()), np.int8), np.ones(len(qu), np.int8)])
-    o = np.lexsort((pu, pi))
+    o = _argsort(pi.astype(np.int64) * U + pu)
     pu, pi, pd_, pr_r, pt = pu[o], pi[o], pd_[o], pr_r[o], pt[o]
     train = Dataset.from_ratings(tu, ti, tr_r, td, U, I, name=f"{spec.name}_train")
     pr = Dataset.from_ratings(pu, pi, pr_r, pd_, U, I, name=f"{spec.name}_pr", is_test=pt)

@@ -260,21 +260,25 @@ __global__ void __launch_bounds__(kThreads) k_user_pass(DeviceState s, EpochPara
 }
 
 // ---------------------------------------------------------------------------
-// Stratified: apply the NSVD1 deltas per item, summed over the item's users
-// in by-item order (apply_nsvd_deltas, src/tsvdx4p.rs:341-385).
+// Stratified: apply the NSVD1 deltas per item (apply_nsvd_deltas,
+// src/tsvdx4p.rs:341-385). The per-item sum over the item's users runs in two
+// fixed-order levels: fixed chunks of kChunkUsers consecutive by-item entries
+// are summed by one warp each (k_y_partial), then each item adds its chunk
+// partials in chunk order (k_y_combine). Same result on every run.
 // ---------------------------------------------------------------------------
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_y_apply(DeviceState s, EpochParams p) {
+__global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s) {
     const int lane = threadIdx.x & 31;
     const uint32_t Fs = s.Fs;
+    constexpr int B = 8;  // rows in flight per warp
     for (;;) {
-        uint32_t k = 0;
-        if (lane == 0) k = atomicAdd(&s.counters[1], 1u);
-        k = __shfl_sync(kFull, k, 0);
-        if (k >= s.n_items) break;
-        const uint32_t i = s.item_work[k];
-        const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
-        if (a == b) continue;
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(&s.counters[1], 1u);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= s.n_chunks) break;
+        const uint64_t a = s.chunk_lo[c];
+        uint64_t b = s.chunk_lo[c + 1];
+        if (b - a > kChunkUsers) b = a + kChunkUsers;
         float acc[VPL];
 #pragma unroll
         for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
@@ -282,17 +286,50 @@ __global__ void __launch_bounds__(kThreads) k_y_apply(DeviceState s, EpochParams
         for (uint64_t base = a; base < b; base += 32) {
             const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
             const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&s.irec[base + lane].key)) : 0u;
-#pragma unroll 4
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const uint32_t u = __shfl_sync(kFull, mine, j);
-                float g[VPL];
-                Row<VPL>::load_nc(s.g_user + (size_t)u * Fs, lane, g);
+            for (uint32_t j = 0; j < cnt; j += B) {
+                float g[B][VPL], e[B];
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) acc[v] += g[v];
-                eacc += __ldg(s.e_user + u);
+                for (int q = 0; q < B; ++q) {
+                    const uint32_t jj = j + q < cnt ? j + q : cnt - 1;
+                    const uint32_t u = __shfl_sync(kFull, mine, jj);
+                    Row<VPL>::load_nc(s.g_user + (size_t)u * Fs, lane, g[q]);
+                    e[q] = __ldg(s.e_user + u);
+                }
+#pragma unroll
+                for (int q = 0; q < B; ++q) {
+                    if (j + q < cnt) {
+#pragma unroll
+                        for (int v = 0; v < VPL; ++v) acc[v] += g[q][v];
+                        eacc += e[q];
+                    }
+                }
             }
         }
-        const float nc = (float)(b - a);
+        Row<VPL>::store(s.chunk_part + (size_t)c * Fs, lane, acc);
+        if (lane == 0) s.chunk_epart[c] = eacc;
+    }
+}
+
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochParams p) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t Fs = s.Fs;
+    const uint32_t warps = gridDim.x * kWarps;
+    for (uint32_t i = blockIdx.x * kWarps + (threadIdx.x >> 5); i < s.n_items; i += warps) {
+        const uint32_t c0 = s.item_chunk0[i], c1 = s.item_chunk0[i + 1];
+        if (c0 == c1) continue;
+        float acc[VPL];
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
+        float eacc = 0.0f;
+        for (uint32_t c = c0; c < c1; ++c) {
+            float g[VPL];
+            Row<VPL>::load_cg(s.chunk_part + (size_t)c * Fs, lane, g);
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) acc[v] += g[v];
+            eacc += __ldcg(s.chunk_epart + c);
+        }
+        const float nc = (float)(s.item_off[i + 1] - s.item_off[i]);
         const float scale = p.nsvd_norm_exp == 0.0f ? 1.0f : powf(nc, p.nsvd_norm_exp);
         float y[VPL];
         Row<VPL>::load_cg(s.yfeat + (size_t)i * Fs, lane, y);
@@ -335,102 +372,239 @@ __global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s) {
 }
 
 // ---------------------------------------------------------------------------
-// Stratified item stratum (fit_epoch_item, src/tsvdx4p.rs:644-762): one warp
-// per item walks the item's ratings in by-item order with the user tables
-// frozen. The item's factor row lives in registers, its NF frequency-bin rows
-// in the warp's shared-memory slice (each lane touches only its own
-// elements), its time- and frequency-bin biases in lane registers.
+// Stratified item stratum (fit_epoch_item, src/tsvdx4p.rs:644-762): items in
+// parallel, each item's ratings in by-item order with the user tables frozen.
+//
+// An item's ratings form a serial chain (every update feeds the next dot
+// product), and the most-rated items carry ~0.5% of all ratings each, so the
+// chain of the hottest item bounds the pass. Items with >= kHeavy ratings get a
+// whole CTA, warp-specialised: warps 1..7 gather the user rows of the next
+// round of kRound ratings from HBM and fold them into
+// pe = (p_u + ycache_u) + dev * p2_u plus the rating's bias scalars in shared
+// memory (double-buffered rounds, one __syncthreads per round), while warp 0
+// runs the chain from shared memory only. Lighter items take one warp each,
+// with the next rating's rows prefetched into registers.
 // ---------------------------------------------------------------------------
+constexpr uint32_t kHeavy = 1024;
+constexpr int kRound = 32;  // ratings per buffered round
+
+struct ItemState {
+    float ib, bt0, bt1, bf0, bf1;
+};
+
+__device__ __forceinline__ ItemState load_item_state(const DeviceState& s, uint32_t i, int lane) {
+    const uint32_t T = s.T, NF = s.NF;
+    ItemState st;
+    st.ib = s.ibias[i];
+    st.bt0 = lane < (int)T ? s.bit_bin[(size_t)i * T + lane] : 0.0f;
+    st.bt1 = lane + 32 < (int)T ? s.bit_bin[(size_t)i * T + 32 + lane] : 0.0f;
+    st.bf0 = lane < (int)NF ? s.ibias_freq[(size_t)i * NF + lane] : 0.0f;
+    st.bf1 = lane + 32 < (int)NF ? s.ibias_freq[(size_t)i * NF + 32 + lane] : 0.0f;
+    return st;
+}
+
+__device__ __forceinline__ void store_item_state(const DeviceState& s, uint32_t i, int lane, const ItemState& st) {
+    const uint32_t T = s.T, NF = s.NF;
+    if (lane == 0) s.ibias[i] = st.ib;
+    if (lane < (int)T) s.bit_bin[(size_t)i * T + lane] = st.bt0;
+    if (lane + 32 < (int)T) s.bit_bin[(size_t)i * T + 32 + lane] = st.bt1;
+    if (lane < (int)NF) s.ibias_freq[(size_t)i * NF + lane] = st.bf0;
+    if (lane + 32 < (int)NF) s.ibias_freq[(size_t)i * NF + 32 + lane] = st.bf1;
+}
+
+// User-side scalars of one by-item rating: bu_t and cu_t (src/tsvdx4p.rs:690-708).
+__device__ __forceinline__ void user_scalars(const DeviceState& s, const Rec& r, float& bu_t, float& cu_t) {
+    const uint32_t u = rec_id(r.key), tb = rec_tbin(r.key);
+    const bool hud = r.ud < s.n_ud;
+    bu_t = __ldg(s.ubias + u) + __ldg(s.but_bin + (size_t)u * s.T + tb) + __ldg(s.alpha_u + u) * r.dev +
+           (hud ? __ldg(s.ubias_day + r.ud) : 0.0f) + __ldg(s.ycache_bias + u);
+    cu_t = __ldg(s.cu + u) + (hud ? __ldg(s.cut + r.ud) : 0.0f);
+}
+
+// One SGD step of the item chain; qf_at(v) is this lane's v-th element of q^f[fb].
+template <int VPL, class QF>
+__device__ __forceinline__ void item_step(const EpochParams& p, float gb, float (&q)[VPL], QF&& qf_at,
+                                          const float (&pe)[VPL], float bu_t, float cu_t, float res, uint32_t tb,
+                                          uint32_t fb, int lane, ItemState& st) {
+    const float bit = __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31);
+    const float ibf = __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
+    const float bi_t = st.ib + bit + ibf;
+    float qfv[VPL], part = 0.0f;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+        qfv[v] = qf_at(v);
+        part += pe[v] * (q[v] + qfv[v]);
+    }
+    const float dot = warp_sum(part);
+    const float err = (gb + bu_t + bi_t * cu_t + dot) - res;
+    const float ec = err * cu_t;
+    st.ib -= p.lr_ib * ec;
+    const float nb = bit - p.lr_ti * ec;
+    if (lane == (int)(tb & 31)) {
+        if (tb < 32) st.bt0 = nb;
+        else st.bt1 = nb;
+    }
+    const float nf = ibf - p.lr_ibf * ec;
+    if (lane == (int)(fb & 31)) {
+        if (fb < 32) st.bf0 = nf;
+        else st.bf1 = nf;
+    }
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+        const float qi = q[v];
+        q[v] = qi - p.lr_i * (err * pe[v] + p.reg_i * qi);
+        qfv[v] = qfv[v] - p.lr_iqf * (err * pe[v] + p.reg_iqf * qfv[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) qf_at(v) = qfv[v];
+}
+
+template <int VPL>
+__device__ void item_light(const DeviceState& s, const EpochParams& p, uint32_t i, int lane) {
+    const uint32_t Fs = s.Fs, NF = s.NF;
+    const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
+    if (a == b) return;
+    float q[VPL];
+    Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
+    ItemState st = load_item_state(s, i, lane);
+    float* qf_base = s.ifeat_freq + (size_t)i * NF * Fs;
+    const float gb = s.gbias;
+    for (uint64_t base = a; base < b; base += 32) {
+        const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+        Rec mine{};
+        if (lane < (int)cnt) mine = load_rec(s.irec + base + lane);
+        float pn[VPL], p2n[VPL], ycn[VPL];
+        {
+            const uint32_t u0 = rec_id(__shfl_sync(kFull, mine.key, 0));
+            Row<VPL>::load_nc(s.ufeat + (size_t)u0 * Fs, lane, pn);
+            Row<VPL>::load_nc(s.ufeat2 + (size_t)u0 * Fs, lane, p2n);
+            Row<VPL>::load_nc(s.ycache + (size_t)u0 * Fs, lane, ycn);
+        }
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const Rec r = shfl_rec(mine, j);
+            float pe[VPL];
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) pe[v] = (pn[v] + ycn[v]) + r.dev * p2n[v];
+            if (j + 1 < cnt) {
+                const uint32_t un = rec_id(__shfl_sync(kFull, mine.key, j + 1));
+                Row<VPL>::load_nc(s.ufeat + (size_t)un * Fs, lane, pn);
+                Row<VPL>::load_nc(s.ufeat2 + (size_t)un * Fs, lane, p2n);
+                Row<VPL>::load_nc(s.ycache + (size_t)un * Fs, lane, ycn);
+            }
+            float bu_t, cu_t;
+            user_scalars(s, r, bu_t, cu_t);
+            const uint32_t tb = rec_tbin(r.key), fb = rec_fbin(r.key);
+            float* qrow = qf_base + (size_t)fb * Fs;
+            float qfv[VPL];
+            Row<VPL>::load_cg(qrow, lane, qfv);
+            item_step<VPL>(p, gb, q, [&](int v) -> float& { return qfv[v]; }, pe, bu_t, cu_t, r.res, tb, fb, lane,
+                           st);
+            Row<VPL>::store(qrow, lane, qfv);
+        }
+    }
+    Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
+    store_item_state(s, i, lane, st);
+}
+
 template <int VPL>
 __global__ void __launch_bounds__(kThreads) k_item_pass(DeviceState s, EpochParams p) {
     extern __shared__ float smem[];
+    __shared__ uint32_t sh_k;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
-    float* qfs = smem + (size_t)warp * NF * Fs;
+    const uint32_t Fs = s.Fs, NF = s.NF;
+    const uint32_t stride = Fs + 4;  // one staged rating: pe row + {bu_t, cu_t, res, key}
+    float* qfs = smem;                                   // [NF][Fs]
+    float* buf = smem + (size_t)NF * Fs;                 // [2][kRound][stride]
     for (;;) {
-        uint32_t k = 0;
-        if (lane == 0) k = atomicAdd(&s.counters[2], 1u);
-        k = __shfl_sync(kFull, k, 0);
-        if (k >= s.n_items) break;
+        if (threadIdx.x == 0) sh_k = atomicAdd(&s.counters[2], 1u);
+        __syncthreads();
+        const uint32_t k = sh_k;
+        __syncthreads();
+        if (k >= s.n_items) return;
         const uint32_t i = s.item_work[k];
         const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
-        if (a == b) continue;
-        float q[VPL];
-        Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
-        for (uint32_t f = 0; f < NF; ++f) {
-            float t[VPL];
-            Row<VPL>::load_cg(s.ifeat_freq + ((size_t)i * NF + f) * Fs, lane, t);
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) qfs[f * Fs + Row<VPL>::elem(lane, v)] = t[v];
+        if (b - a < kHeavy) {
+            // Items are ordered heaviest first: from here on every item is light.
+            if (warp == 0) item_light<VPL>(s, p, i, lane);
+            for (;;) {
+                uint32_t k2 = 0;
+                if (lane == 0) k2 = atomicAdd(&s.counters[2], 1u);
+                k2 = __shfl_sync(kFull, k2, 0);
+                if (k2 >= s.n_items) return;
+                item_light<VPL>(s, p, s.item_work[k2], lane);
+            }
         }
-        float ib = s.ibias[i];
-        float bt0 = lane < (int)T ? s.bit_bin[(size_t)i * T + lane] : 0.0f;
-        float bt1 = lane + 32 < (int)T ? s.bit_bin[(size_t)i * T + 32 + lane] : 0.0f;
-        float bf0 = lane < (int)NF ? s.ibias_freq[(size_t)i * NF + lane] : 0.0f;
-        float bf1 = lane + 32 < (int)NF ? s.ibias_freq[(size_t)i * NF + 32 + lane] : 0.0f;
-        const float gb = s.gbias;
-        for (uint64_t base = a; base < b; base += 32) {
-            const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
-            Rec mine{};
-            if (lane < (int)cnt) mine = load_rec(s.irec + base + lane);
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const Rec r = shfl_rec(mine, j);
-                const uint32_t u = rec_id(r.key), tb = rec_tbin(r.key), fb = rec_fbin(r.key);
-                float pu[VPL], p2[VPL], yc[VPL];
+        // ---------------- heavy item: whole CTA ----------------
+        for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
+            qfs[e] = __ldcg(s.ifeat_freq + (size_t)i * NF * Fs + e);
+        const uint64_t n = b - a;
+        const uint32_t rounds = (uint32_t)((n + kRound - 1) / kRound);
+        float q[VPL];
+        ItemState st{};
+        if (warp == 0) {
+            Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
+            st = load_item_state(s, i, lane);
+        }
+        // producers fill round r into buffer r & 1
+        auto produce = [&](uint32_t r) {
+            float* dst = buf + (size_t)(r & 1) * kRound * stride;
+            const uint64_t r0 = a + (uint64_t)r * kRound;
+            const uint64_t left = n - (uint64_t)r * kRound;
+            const uint32_t m = (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
+            for (uint32_t j = warp - 1; j < m; j += kWarps - 1) {
+                const Rec rr = load_rec(s.irec + r0 + j);
+                const uint32_t u = rec_id(rr.key);
+                float pu[VPL], p2[VPL], yc[VPL], pe[VPL];
                 Row<VPL>::load_nc(s.ufeat + (size_t)u * Fs, lane, pu);
                 Row<VPL>::load_nc(s.ufeat2 + (size_t)u * Fs, lane, p2);
                 Row<VPL>::load_nc(s.ycache + (size_t)u * Fs, lane, yc);
-                const float dv = r.dev;
-                const float bu_t = __ldg(s.ubias + u) + __ldg(s.but_bin + (size_t)u * T + tb) + __ldg(s.alpha_u + u) * dv +
-                                   (r.ud < s.n_ud ? __ldg(s.ubias_day + r.ud) : 0.0f) + __ldg(s.ycache_bias + u);
-                const float bit = __shfl_sync(kFull, tb < 32 ? bt0 : bt1, tb & 31);
-                const float ibf = __shfl_sync(kFull, fb < 32 ? bf0 : bf1, fb & 31);
-                const float bi_t = ib + bit + ibf;
-                const float cu_t = __ldg(s.cu + u) + (r.ud < s.n_ud ? __ldg(s.cut + r.ud) : 0.0f);
-                float* qrow = qfs + fb * Fs;
-                float pe[VPL], part = 0.0f;
+                float bu_t, cu_t;
+                user_scalars(s, rr, bu_t, cu_t);
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) {
-                    pe[v] = (pu[v] + yc[v]) + dv * p2[v];
-                    part += pe[v] * (q[v] + qrow[Row<VPL>::elem(lane, v)]);
-                }
-                const float dot = warp_sum(part);
-                const float err = (gb + bu_t + bi_t * cu_t + dot) - r.res;
-                const float ec = err * cu_t;
-                ib -= p.lr_ib * ec;
-                {
-                    const float nb = bit - p.lr_ti * ec;
-                    if (lane == (int)(tb & 31)) {
-                        if (tb < 32) bt0 = nb;
-                        else bt1 = nb;
-                    }
-                    const float nf = ibf - p.lr_ibf * ec;
-                    if (lane == (int)(fb & 31)) {
-                        if (fb < 32) bf0 = nf;
-                        else bf1 = nf;
-                    }
-                }
+                for (int v = 0; v < VPL; ++v) pe[v] = (pu[v] + yc[v]) + rr.dev * p2[v];
+                float* row = dst + (size_t)j * stride;
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) {
-                    const int e = Row<VPL>::elem(lane, v);
-                    const float qi = q[v], qfk = qrow[e];
-                    q[v] = qi - p.lr_i * (err * pe[v] + p.reg_i * qi);
-                    qrow[e] = qfk - p.lr_iqf * (err * pe[v] + p.reg_iqf * qfk);
+                for (int v = 0; v < VPL; ++v) row[Row<VPL>::elem(lane, v)] = pe[v];
+                if (lane == 0) {
+                    row[Fs] = bu_t;
+                    row[Fs + 1] = cu_t;
+                    row[Fs + 2] = rr.res;
+                    row[Fs + 3] = __uint_as_float(rr.key);
                 }
             }
-        }
-        Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
-        for (uint32_t f = 0; f < NF; ++f) {
-            float t[VPL];
+        };
+        if (warp > 0) produce(0);
+        __syncthreads();
+        const float gb = s.gbias;
+        for (uint32_t r = 0; r < rounds; ++r) {
+            if (warp > 0) {
+                if (r + 1 < rounds) produce(r + 1);
+            } else {
+                const float* src = buf + (size_t)(r & 1) * kRound * stride;
+                const uint64_t left = n - (uint64_t)r * kRound;
+                const uint32_t m = (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
+                for (uint32_t j = 0; j < m; ++j) {
+                    const float* row = src + (size_t)j * stride;
+                    float pe[VPL];
 #pragma unroll
-            for (int v = 0; v < VPL; ++v) t[v] = qfs[f * Fs + Row<VPL>::elem(lane, v)];
-            Row<VPL>::store(s.ifeat_freq + ((size_t)i * NF + f) * Fs, lane, t);
+                    for (int v = 0; v < VPL; ++v) pe[v] = row[Row<VPL>::elem(lane, v)];
+                    const float bu_t = row[Fs], cu_t = row[Fs + 1], res = row[Fs + 2];
+                    const uint32_t key = __float_as_uint(row[Fs + 3]);
+                    const uint32_t tb = rec_tbin(key), fb = rec_fbin(key);
+                    float* qrow = qfs + (size_t)fb * Fs;
+                    item_step<VPL>(p, gb, q, [&](int v) -> float& { return qrow[Row<VPL>::elem(lane, v)]; }, pe,
+                                   bu_t, cu_t, res, tb, fb, lane, st);
+                }
+            }
+            __syncthreads();
         }
-        if (lane == 0) s.ibias[i] = ib;
-        if (lane < (int)T) s.bit_bin[(size_t)i * T + lane] = bt0;
-        if (lane + 32 < (int)T) s.bit_bin[(size_t)i * T + 32 + lane] = bt1;
-        if (lane < (int)NF) s.ibias_freq[(size_t)i * NF + lane] = bf0;
-        if (lane + 32 < (int)NF) s.ibias_freq[(size_t)i * NF + 32 + lane] = bf1;
+        if (warp == 0) {
+            Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
+            store_item_state(s, i, lane, st);
+        }
+        for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
+            __stcg(s.ifeat_freq + (size_t)i * NF * Fs + e, qfs[e]);
+        __syncthreads();
     }
 }
 
@@ -462,10 +636,13 @@ void launch_user_pass(tsvd_model* m, const EpochParams& p, const uint32_t* order
 
 template <int VPL>
 void launch_y_apply(tsvd_model* m, const EpochParams& p) {
-    unsigned g = persistent_grid(k_y_apply<VPL>, 0);
-    k_y_apply<VPL><<<g, kThreads, 0, m->stream>>>(m->d, p);
+    unsigned g = persistent_grid(k_y_partial<VPL>, 0);
+    k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(m->d);
     TSVD_CUDA(cudaGetLastError());
-    m->launches++;
+    unsigned g2 = ceil_div(m->d.n_items, kWarps);
+    k_y_combine<VPL><<<g2, kThreads, 0, m->stream>>>(m->d, p);
+    TSVD_CUDA(cudaGetLastError());
+    m->launches += 2;
 }
 
 template <int VPL>
@@ -478,7 +655,7 @@ void launch_rebuild(tsvd_model* m) {
 
 template <int VPL>
 void launch_item_pass(tsvd_model* m, const EpochParams& p) {
-    size_t smem = (size_t)kWarps * m->d.NF * m->d.Fs * sizeof(float);
+    size_t smem = ((size_t)m->d.NF * m->d.Fs + 2ull * kRound * (m->d.Fs + 4)) * sizeof(float);
     TSVD_CUDA(cudaFuncSetAttribute(k_item_pass<VPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     unsigned g = persistent_grid(k_item_pass<VPL>, smem);
     k_item_pass<VPL><<<g, kThreads, smem, m->stream>>>(m->d, p);

@@ -64,6 +64,7 @@ struct __align__(16) Rec {
     uint32_t ud;
 };
 constexpr uint32_t kIdBits = 20, kIdMask = (1u << kIdBits) - 1u;
+constexpr uint32_t kChunkUsers = 512;  // ratings per chunk of the by-item split sums
 constexpr uint32_t kMaxBins = 64;
 
 // Kernel arguments for one model (everything a kernel may touch).
@@ -100,6 +101,12 @@ struct DeviceState {
     const uint32_t* user_work;  // users in processing order
     const uint32_t* item_work;  // items in processing order
     uint32_t* counters;         // [8] dynamic work counters
+    // fixed-size chunks of the by-item index (deterministic split reductions)
+    uint32_t n_chunks;
+    const uint64_t* chunk_lo;      // [n_chunks + 1] start of each chunk in irec; last = n_train
+    const uint32_t* item_chunk0;   // [I+1] first chunk of each item
+    float* chunk_part;             // [n_chunks, Fs] partial sums
+    float* chunk_epart;            // [n_chunks]
 };
 
 struct KernelStat {
@@ -129,6 +136,7 @@ struct tsvd_model {
     tsvd::DevMem m_alpha_u, m_but_bin, m_bit_bin, m_ybias, m_ycache_bias;
     tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
     tsvd::DevMem m_g_user, m_e_user, m_user_work, m_item_work, m_counters;
+    tsvd::DevMem m_chunk_lo, m_item_chunk0, m_chunk_part, m_chunk_epart;
     tsvd::DevMem m_perm;          // [U] epoch order upload buffer
     tsvd::DevMem m_scratch;       // predict / rmse scratch
     size_t scratch_rows = 0;

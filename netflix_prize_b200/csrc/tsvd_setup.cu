@@ -328,6 +328,24 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         upload(m->m_user_work, uw.data(), U, st);
         s.item_work = m->m_item_work.as<uint32_t>();
         s.user_work = m->m_user_work.as<uint32_t>();
+        // fixed chunks of kChunkUsers ratings per item (deterministic split sums)
+        std::vector<uint64_t> clo;
+        std::vector<uint32_t> c0(I + 1, 0);
+        for (uint32_t i = 0; i < I; ++i) {
+            c0[i] = (uint32_t)clo.size();
+            for (uint64_t a = ioff[i]; a < ioff[i + 1]; a += kChunkUsers) clo.push_back(a);
+        }
+        c0[I] = (uint32_t)clo.size();
+        s.n_chunks = (uint32_t)clo.size();
+        clo.push_back(R);
+        upload(m->m_chunk_lo, clo.data(), clo.size(), st);
+        upload(m->m_item_chunk0, c0.data(), c0.size(), st);
+        m->m_chunk_part.alloc((size_t)s.n_chunks * Fs * 4);
+        m->m_chunk_epart.alloc((size_t)s.n_chunks * 4);
+        s.chunk_lo = m->m_chunk_lo.as<uint64_t>();
+        s.item_chunk0 = m->m_item_chunk0.as<uint32_t>();
+        s.chunk_part = m->m_chunk_part.as<float>();
+        s.chunk_epart = m->m_chunk_epart.as<float>();
         TSVD_CUDA(cudaStreamSynchronize(st));
     }
 

@@ -48,6 +48,8 @@ def parse_args():
     ap.add_argument("--f", type=int, default=256)
     ap.add_argument("--shape", choices=["c2", "c1", "c3"], default="c2")
     ap.add_argument("--schedule", choices=["hogwild", "stratified"], default="hogwild")
+    ap.add_argument("--precision", choices=["fp32", "bf16", "bf16all"], default="fp32",
+                    help="BF16 read copies (stratified only): item and y tables, or also user rows")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sample-users", type=int, default=20000, help="users in the CPU sample")
@@ -197,9 +199,9 @@ def run_reference(args):
 def workload_config(args):
     spec = spec_for(args.shape)
     return {"workload": f"tsvdx4 lm preset, {args.shape} shape ({spec.n_users} users x {spec.n_items} items, "
-                        f"{spec.n_train} ratings), f={args.f}, T=30, low_memory, schedule={args.schedule}",
+                        f"{spec.n_train} ratings), f={args.f}, T=30, low_memory, schedule={args.schedule}, precision={args.precision}",
             "n_feat": args.f, "n_users": spec.n_users, "n_items": spec.n_items, "n_ratings": spec.n_train,
-            "schedule": args.schedule,
+            "schedule": args.schedule, "precision": args.precision,
             "l2": "inputs larger than L2 (16-byte rating records: 1.6 GB per epoch at the c2 shape)"}
 
 
@@ -241,6 +243,7 @@ def main():
     from netflix_prize_b200.model import TxModel
 
     sched = SCHED_HOGWILD if args.schedule == "hogwild" else SCHED_STRATIFIED
+    prec = {"fp32": 0, "bf16": 1, "bf16all": 2}[args.precision]
     spec = spec_for(args.shape)
     tr, pr = synth.generate(spec)
     R = tr.n_ratings
@@ -260,7 +263,7 @@ def main():
 
     stream = torch.cuda.current_stream()
     # ---------------- value: device-resident epochs ----------------
-    model = TxModel(tr, MaskedDataset(pr), cfg, schedule=sched, device=local)
+    model = TxModel(tr, MaskedDataset(pr), cfg, schedule=sched, precision=prec, device=local)
     model.set_stream(stream.cuda_stream)
     for e in range(1, args.warmup + 1):
         model.fit_epoch(tr, pr, e)
@@ -313,7 +316,7 @@ def main():
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        m2 = TxModel(trp, MaskedDataset(prp), cfg, schedule=sched, device=local)
+        m2 = TxModel(trp, MaskedDataset(prp), cfg, schedule=sched, precision=prec, device=local)
         m2.set_stream(stream.cuda_stream)
         e2e_rmse = None
         for k in range(args.steps):

@@ -115,9 +115,15 @@ enum tsvd_schedule {
     TSVD_SCHED_STRATIFIED = 1
 };
 
+/* Precision forms (stratified schedule only: its strata read frozen tables).
+ * Masters are FP32 in every form; accumulation is FP32; the global mean and
+ * the SSE/RMSE reductions are FP64. */
 enum tsvd_precision {
-    TSVD_PREC_FP32 = 0,     /* all reads and writes FP32                     */
-    TSVD_PREC_BF16_READ = 1 /* FP32 masters; BF16 read copies of q_i and y_j */
+    TSVD_PREC_FP32 = 0,         /* all reads FP32                                */
+    TSVD_PREC_BF16_READ = 1,    /* BF16 read copies of the item tables q_i,
+                                   q^f_i and of y_j, refreshed each stratum      */
+    TSVD_PREC_BF16_READ_ALL = 2 /* also BF16 copies of the user rows p_u, p2_u,
+                                   ycache_u that the item stratum gathers        */
 };
 
 /* Options that have no counterpart in TxConfig. Zero-initialised = defaults. */
@@ -210,6 +216,79 @@ int tsvd_get_user_order(const tsvd_model* m, uint64_t epoch, uint32_t* perm, uin
  * (src/lib.rs:64-67). */
 int tsvd_user_order_for_seed(uint64_t n, int32_t shuffle, uint64_t seed, uint64_t epoch, uint32_t* perm);
 int tsvd_normal_stream(uint64_t seed, float sigma, uint64_t n, float* out);
+
+/* ---- batched form: several variants in one persistent launch ---------- */
+
+/* A group of variants over one dataset, e.g. the lr/reg/n_feat grid of a
+ * hyperparameter search. Each variant is a TxModel (src/tx.rs:457-1116) with
+ * its own parameters and Hogwild epochs (its own get_users order); the data
+ * are held once. Variants must share n_time_bins, n_freq_bins, beta,
+ * low_memory and full_su. opts must select Hogwild / FP32. */
+typedef struct tsvd_group tsvd_group;
+int tsvd_group_create(const tsvd_config* cfgs, uint32_t n_models,
+                      const tsvd_gpu_options* opts, const tsvd_dataset_view* tr,
+                      const tsvd_dataset_view* pr_masked, tsvd_group** out);
+void tsvd_group_destroy(tsvd_group* g);
+int tsvd_group_size(const tsvd_group* g, uint32_t* out);
+/* Borrowed model k: predict/rmse/get_param/set_param work on it; it must not
+ * be destroyed by the caller and lives as long as the group. */
+int tsvd_group_model(tsvd_group* g, uint32_t k, tsvd_model** out);
+/* One epoch of every variant: one persistent launch plus one batched ycache
+ * rebuild; from the second epoch on they replay one captured CUDA graph. */
+int tsvd_group_fit_epoch(tsvd_group* g, uint64_t epoch);
+/* 0 = launch directly every epoch (no CUDA graph). */
+int tsvd_group_set_graphs(tsvd_group* g, int32_t enabled);
+/* Device time of the last group epoch (CUDA events around the launch). */
+int tsvd_group_last_epoch_ms(const tsvd_group* g, double* out);
+/* Picks the Hogwild prefetch depth (2..4 staged ratings) per feature width by
+ * timing each candidate on throwaway parameter copies over the units of the
+ * sample_users heaviest users; chosen_stages (n_models ints) may be NULL. */
+int tsvd_group_autotune(tsvd_group* g, uint32_t sample_users, int32_t* chosen_stages);
+const char* tsvd_group_last_error(const tsvd_group* g);
+
+/* ---- learned warm start: amortised user encoder + fold-in --------------- */
+
+/* No counterpart in the reference. An encoder predicts a user's p_u, b_u and
+ * alpha_u from the user's training history (embedding bag over item, rating
+ * and time bin, dim 128; MLP 128 -> 512 -> 512 -> f+2 with GELU; BF16
+ * tensor-core GEMMs, FP32 accumulation, FP32 master weights, AdamW). Targets
+ * are the current factors of model m for the target users, standardised per
+ * dimension with statistics of target_users. train_raw is the training set's
+ * raw_ratings column (n_train entries, values 1..5). */
+typedef struct tsvd_encoder tsvd_encoder;
+int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw,
+                        const uint32_t* target_users, uint64_t n_target,
+                        uint64_t seed, float lr, float weight_decay,
+                        tsvd_encoder** out);
+void tsvd_encoder_destroy(tsvd_encoder* e);
+/* One pass over users in mini-batches of `batch` (<= 4096): forward, MSE,
+ * backward, AdamW step. */
+int tsvd_encoder_train_epoch(tsvd_encoder* e, const uint32_t* users, uint64_t n,
+                             uint32_t batch, double* mean_loss);
+/* Loss and gradients of one batch (n <= 4096) without an update; gradients
+ * are read with tsvd_encoder_get("g.<name>"). */
+int tsvd_encoder_loss_grad(tsvd_encoder* e, const uint32_t* users, uint32_t n, double* loss);
+/* Standardised outputs [n, f+2] (n <= 4096). */
+int tsvd_encoder_forward(tsvd_encoder* e, const uint32_t* users, uint32_t n, float* out);
+/* Writes de-standardised predictions of p_u, b_u, alpha_u into model m for
+ * `users` and resets their other user state to the standard init. */
+int tsvd_encoder_apply(tsvd_encoder* e, tsvd_model* m, const uint32_t* users, uint64_t n);
+/* Parameters (or gradients as "g.<name>"): e_item, e_rate, e_date, w1, b1,
+ * w2, b2, w3, b3; FP32, matrices [in, out] row-major. */
+int tsvd_encoder_get(const tsvd_encoder* e, const char* name, float* dst, uint64_t count);
+int tsvd_encoder_set(tsvd_encoder* e, const char* name, const float* src, uint64_t count);
+int tsvd_encoder_target_stats(const tsvd_encoder* e, float* mean, float* std_out);
+const char* tsvd_encoder_last_error(const tsvd_encoder* e);
+
+/* Fold-in: `passes` user-side SGD passes over `users` with every item-side
+ * table frozen -- the user phase of the reference's parallel schedule
+ * (src/tsvdx4p.rs:390-639) restricted to those users, without the NSVD1
+ * delta step. */
+int tsvd_foldin(tsvd_model* m, const uint32_t* users, uint64_t n, uint32_t passes);
+
+/* Standard init of `users`' state (p_u ~ N(0, sigma_u) from StdRng(seed),
+ * everything else as TxModel::new sets it), for fold-in baselines. */
+int tsvd_reset_users(tsvd_model* m, const uint32_t* users, uint64_t n, uint64_t seed);
 
 /* ---- streams, timing, errors ------------------------------------------ */
 

@@ -20,6 +20,7 @@ SCHED_HOGWILD = 0
 SCHED_STRATIFIED = 1
 PREC_FP32 = 0
 PREC_BF16_READ = 1
+PREC_BF16_READ_ALL = 2
 
 
 class TsvdOrdinalConfig(C.Structure):

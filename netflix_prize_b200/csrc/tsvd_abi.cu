@@ -133,8 +133,11 @@ int tsvd_create(const tsvd_config* cfg, const tsvd_gpu_options* opts, const tsvd
         }
         if (m->opts.schedule != TSVD_SCHED_HOGWILD && m->opts.schedule != TSVD_SCHED_STRATIFIED)
             throw Error(TSVD_ERR_INVALID, "unknown schedule");
-        if (m->opts.precision != TSVD_PREC_FP32)
-            throw Error(TSVD_ERR_UNSUPPORTED, "only FP32 precision is built so far");
+        if (m->opts.precision < TSVD_PREC_FP32 || m->opts.precision > TSVD_PREC_BF16_READ_ALL)
+            throw Error(TSVD_ERR_INVALID, "unknown precision");
+        if (m->opts.precision != TSVD_PREC_FP32 && m->opts.schedule != TSVD_SCHED_STRATIFIED)
+            throw Error(TSVD_ERR_UNSUPPORTED,
+                        "BF16 read copies need the stratified schedule (Hogwild writes the tables it reads)");
         int n_dev = 0;
         if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
             throw Error(TSVD_ERR_NO_DEVICE, "no CUDA device is visible");
@@ -286,6 +289,7 @@ int tsvd_param_nbytes(const tsvd_model* m, const char* name, uint64_t* out) {
     return guarded(m, [&] {
         std::string n(name);
         if (n == "gbias") { *out = 4; return; }
+        if (n == "thresholds" && m->cfg.has_ordinal_head) { *out = 16; return; }
         ParamRef r;
         if (!find_param(m, n, r)) throw Error(TSVD_ERR_INVALID, "unknown or unavailable parameter " + n);
         *out = r.rows * r.cols * 4;
@@ -301,6 +305,12 @@ int tsvd_get_param(const tsvd_model* m, const char* name, void* dst, uint64_t nb
         if (n == "gbias") {
             if (nbytes != 4) throw Error(TSVD_ERR_INVALID, "gbias is 4 bytes");
             std::memcpy(dst, &m->d.gbias, 4);
+            return;
+        }
+        if (n == "thresholds") {
+            if (!m->cfg.has_ordinal_head) throw Error(TSVD_ERR_INVALID, "the model has no ordinal head");
+            if (nbytes != 16) throw Error(TSVD_ERR_INVALID, "thresholds are 16 bytes");
+            std::memcpy(dst, m->h_thresholds, 16);
             return;
         }
         ParamRef r;

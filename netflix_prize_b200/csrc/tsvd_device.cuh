@@ -132,6 +132,42 @@ __device__ __forceinline__ float dev_of(int32_t day, float tu_mean, float beta) 
     return s * powf(fabsf(dt), beta);
 }
 
+// OrdinalHead (src/lib.rs:500-609): P(Y <= k) = sigmoid(th[k-1] - score).
+__device__ __forceinline__ float sigmoid_f(float x) { return 1.0f / (1.0f + expf(-x)); }
+
+// d(-log P(Y = y)) / d(score), y in 1..5 (OrdinalHead::grad, src/lib.rs:562-598)
+__device__ __forceinline__ float ordinal_grad(const float (&th)[4], float score, int y) {
+    float f[6], a[6];
+    f[0] = 0.0f;
+    f[5] = 1.0f;
+#pragma unroll
+    for (int k = 1; k < 5; ++k) f[k] = sigmoid_f(th[k - 1] - score);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) a[k] = f[k] * (1.0f - f[k]);
+    float fy = f[1], fy1 = f[0], ay = a[1], ay1 = a[0];
+#pragma unroll
+    for (int k = 2; k <= 5; ++k)
+        if (y == k) {
+            fy = f[k];
+            fy1 = f[k - 1];
+            ay = a[k];
+            ay1 = a[k - 1];
+        }
+    const float p_y = fmaxf(fy - fy1, 1e-6f);
+    return (ay - ay1) / p_y;
+}
+
+// E[r] = sum_k k P(Y = k) (TxModel::predict with the head, src/tx.rs:716-722)
+__device__ __forceinline__ float ordinal_expect(const float* th, float score) {
+    float f[6];
+    f[0] = 0.0f;
+    f[5] = 1.0f;
+#pragma unroll
+    for (int k = 1; k < 5; ++k) f[k] = sigmoid_f(th[k - 1] - score);
+    return 1.0f * (f[1] - f[0]) + 2.0f * (f[2] - f[1]) + 3.0f * (f[3] - f[2]) + 4.0f * (f[4] - f[3]) +
+           5.0f * (f[5] - f[4]);
+}
+
 // freq_bin (src/tx.rs:87-90)
 __device__ __forceinline__ uint32_t freq_bin(uint32_t day_cnt, uint32_t NF) {
     if (day_cnt <= 1) return 0;
@@ -152,6 +188,62 @@ __device__ __forceinline__ uint32_t ud_index(const DeviceState& s, uint32_t u, i
     }
     if (lo < s.ud_start[u + 1] && s.ud_date[lo] == day) return (uint32_t)lo;
     return 0xffffffffu;
+}
+
+}  // namespace tsvd
+
+namespace tsvd {
+
+// ---- asynchronous global -> shared copies (cp.async); each lane copies and
+// later reads only its own elements, so a lane's own wait_group suffices.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copy this lane's elements of a feature row into a shared-memory row with the
+// same layout, and read them back.
+template <int VPL>
+__device__ __forceinline__ void row_cp_async(float* srow, const float* grow, int lane) {
+    if constexpr (VPL % 4 == 0) {
+#pragma unroll
+        for (int c = 0; c < VPL / 4; ++c) cp_async16(srow + c * 128 + lane * 4, grow + c * 128 + lane * 4);
+    } else if constexpr (VPL == 2) {
+        cp_async8(srow + lane * 2, grow + lane * 2);
+    } else {
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) cp_async4(srow + v * 32 + lane, grow + v * 32 + lane);
+    }
+}
+
+template <int VPL>
+__device__ __forceinline__ void row_from_smem(const float* srow, int lane, float (&x)[VPL]) {
+    if constexpr (VPL % 4 == 0) {
+#pragma unroll
+        for (int c = 0; c < VPL / 4; ++c) {
+            const float4 t = *reinterpret_cast<const float4*>(srow + c * 128 + lane * 4);
+            x[4 * c] = t.x; x[4 * c + 1] = t.y; x[4 * c + 2] = t.z; x[4 * c + 3] = t.w;
+        }
+    } else if constexpr (VPL == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(srow + lane * 2);
+        x[0] = t.x; x[1] = t.y;
+    } else {
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) x[v] = srow[v * 32 + lane];
+    }
 }
 
 }  // namespace tsvd

@@ -1,0 +1,721 @@
+// Learned warm start: an amortised user encoder that predicts a user's
+// factors (p_u, b_u, alpha_u) from the user's rating history, to initialise
+// fold-in of new users instead of the standard init (p_u ~ N(0, sigma_u),
+// b_u = alpha_u = 0). There is no counterpart in the reference; the fold-in
+// itself is the reference's user-side SGD with item tables frozen
+// (src/tsvdx4p.rs:390-639).
+//
+//   h0 = mean over the user's training ratings of
+//        E_item[i] + E_rating[r - 1] + E_date[time_bin(t)]          (dim 128)
+//   h1 = GELU(h0 W1 + b1)   128 -> 512
+//   h2 = GELU(h1 W2 + b2)   512 -> 512
+//   y  = h2 W3 + b3         512 -> f + 2   (standardised p_u, b_u, alpha_u)
+//
+// Loss: mean squared error against the standardised targets. Weights are FP32
+// masters with BF16 copies; every GEMM runs on the tensor cores with BF16
+// operands and FP32 accumulation (mma.sync m16n8k16), activations are stored
+// as BF16 for the next GEMM and as FP32 pre-activations for the GELU
+// derivative. AdamW updates all parameters (weight decay on the matrices).
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rand_stream.hpp"
+#include "tsvd_epoch.cuh"
+
+using tsvd::Error;
+
+namespace tsvd {
+namespace {
+
+constexpr int kEmb = 128, kHid = 512, kMaxBatch = 4096;
+
+// ---------------------------------------------------------------------------
+// C[M,N] = op(A)[M,K] . op(B)[K,N] with BF16 operands, FP32 accumulation.
+// A is [M,K] row-major (a_km = 0) or stored as [K,M] (a_km = 1); B is stored
+// as [K,N] (b_kn = 1) or [N,K] (b_kn = 0). 64x64 tiles, BK = 32, 4 warps of
+// 32x32, operands staged in shared memory as [64][BK] rows (B transposed) and
+// fed to mma.sync through ldmatrix.
+// Epilogue: + bias[n] (optional); out_f32 and/or out_bf16 (optional); with
+// gelu, out_f32 receives the pre-activation and out_bf16 GELU of it.
+// ---------------------------------------------------------------------------
+constexpr int TM = 64, TN = 64, TK = 32, TKP = TK + 8;
+
+struct GemmArgs {
+    const __nv_bfloat16* A;
+    const __nv_bfloat16* B;
+    int M, N, K, lda, ldb, a_km, b_kn;
+    const float* bias;
+    float* out_f32;
+    __nv_bfloat16* out_bf16;
+    int ldc, gelu;
+};
+
+__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+    return cdf + x * pdf;
+}
+
+__device__ __forceinline__ void ldmatrix_x4(unsigned (&r)[4], const void* p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+__device__ __forceinline__ void ldmatrix_x2(unsigned (&r)[2], const void* p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
+    __shared__ __align__(16) __nv_bfloat16 As[TM][TKP];
+    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TKP];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    for (int k0 = 0; k0 < g.K; k0 += TK) {
+        for (int e = tid; e < TM * TK; e += 128) {
+            const int r = e / TK, c = e % TK;
+            const int gm = m0 + r, gk = k0 + c;
+            __nv_bfloat16 v = zero;
+            if (gm < g.M && gk < g.K) v = g.a_km ? g.A[(size_t)gk * g.lda + gm] : g.A[(size_t)gm * g.lda + gk];
+            As[r][c] = v;
+        }
+        for (int e = tid; e < TN * TK; e += 128) {
+            const int r = e / TK, c = e % TK;
+            const int gn = n0 + r, gk = k0 + c;
+            __nv_bfloat16 v = zero;
+            if (gn < g.N && gk < g.K) v = g.b_kn ? g.B[(size_t)gk * g.ldb + gn] : g.B[(size_t)gn * g.ldb + gk];
+            Bs[r][c] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; kk += 16) {
+            unsigned af[2][4], bfr[4][2];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int row = wm + a * 16 + (lane & 15);
+                const int col = kk + ((lane >> 4) << 3);
+                ldmatrix_x4(af[a], &As[row][col]);
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int row = wn + b * 8 + (lane & 7);
+                const int col = kk + (((lane >> 3) & 1) << 3);
+                ldmatrix_x2(bfr[b], &Bs[row][col]);
+            }
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) mma_bf16(acc[a][b], af[a], bfr[b]);
+        }
+        __syncthreads();
+    }
+    // accumulator layout of m16n8: c0,c1 -> row lane/4, cols 2*(lane%4)+{0,1}; c2,c3 -> row lane/4 + 8
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int m = m0 + wm + a * 16 + (lane >> 2) + h * 8;
+                    const int n = n0 + wn + b * 8 + 2 * (lane & 3) + c;
+                    if (m >= g.M || n >= g.N) continue;
+                    float v = acc[a][b][h * 2 + c];
+                    if (g.bias) v += g.bias[n];
+                    if (g.out_f32) g.out_f32[(size_t)m * g.ldc + n] = v;
+                    if (g.out_bf16) g.out_bf16[(size_t)m * g.ldc + n] = __float2bfloat16(g.gelu ? gelu_f(v) : v);
+                }
+}
+
+void gemm(cudaStream_t st, const __nv_bfloat16* A, int a_km, int lda, const __nv_bfloat16* B, int b_kn, int ldb, int M,
+          int N, int K, const float* bias, float* out_f32, __nv_bfloat16* out_bf16, int ldc, int gelu) {
+    GemmArgs g{A, B, M, N, K, lda, ldb, a_km, b_kn, bias, out_f32, out_bf16, ldc, gelu};
+    dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
+    k_gemm_bf16<<<grid, 128, 0, st>>>(g);
+    TSVD_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Embedding bag over a batch of users: warp per user, 4 of the 128 dims per
+// lane. Emits FP32 and BF16 copies of h0.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_embag_fwd(DeviceState s, const int8_t* __restrict__ raw,
+                                                   const uint32_t* __restrict__ users, int n,
+                                                   const float* __restrict__ e_item, const float* __restrict__ e_rate,
+                                                   const float* __restrict__ e_date, float* __restrict__ h0,
+                                                   __nv_bfloat16* __restrict__ h0b) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (w >= n) return;
+    const uint32_t u = users[w];
+    const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint64_t t = a; t < b; ++t) {
+        const Rec r = load_rec(s.rec + t);
+        const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+        const int rt = min(max((int)raw[t], 1), 5) - 1;
+        const float4 x = __ldg(reinterpret_cast<const float4*>(e_item + (size_t)i * kEmb) + lane);
+        const float4 y = __ldg(reinterpret_cast<const float4*>(e_rate + (size_t)rt * kEmb) + lane);
+        const float4 z = __ldg(reinterpret_cast<const float4*>(e_date + (size_t)tb * kEmb) + lane);
+        acc.x += x.x + y.x + z.x;
+        acc.y += x.y + y.y + z.y;
+        acc.z += x.z + y.z + z.z;
+        acc.w += x.w + y.w + z.w;
+    }
+    const float inv = b > a ? 1.0f / (float)(b - a) : 0.0f;
+    acc.x *= inv; acc.y *= inv; acc.z *= inv; acc.w *= inv;
+    reinterpret_cast<float4*>(h0 + (size_t)w * kEmb)[lane] = acc;
+    __nv_bfloat16* o = h0b + (size_t)w * kEmb + 4 * lane;
+    o[0] = __float2bfloat16(acc.x); o[1] = __float2bfloat16(acc.y);
+    o[2] = __float2bfloat16(acc.z); o[3] = __float2bfloat16(acc.w);
+}
+
+// dE += dh0 / n_u for every rating of every user in the batch (atomics: users
+// share items).
+__global__ void __launch_bounds__(256) k_embag_bwd(DeviceState s, const int8_t* __restrict__ raw,
+                                                   const uint32_t* __restrict__ users, int n,
+                                                   const float* __restrict__ dh0, float* __restrict__ g_item,
+                                                   float* __restrict__ g_rate, float* __restrict__ g_date) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (w >= n) return;
+    const uint32_t u = users[w];
+    const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
+    if (a == b) return;
+    const float inv = 1.0f / (float)(b - a);
+    float4 d = reinterpret_cast<const float4*>(dh0 + (size_t)w * kEmb)[lane];
+    d.x *= inv; d.y *= inv; d.z *= inv; d.w *= inv;
+    float4 rs[5];
+    for (int q = 0; q < 5; ++q) rs[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint64_t t = a; t < b; ++t) {
+        const Rec r = load_rec(s.rec + t);
+        const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+        const int rt = min(max((int)raw[t], 1), 5) - 1;
+        float* gi = g_item + (size_t)i * kEmb + 4 * lane;
+        atomicAdd(gi, d.x); atomicAdd(gi + 1, d.y); atomicAdd(gi + 2, d.z); atomicAdd(gi + 3, d.w);
+        float* gd = g_date + (size_t)tb * kEmb + 4 * lane;
+        atomicAdd(gd, d.x); atomicAdd(gd + 1, d.y); atomicAdd(gd + 2, d.z); atomicAdd(gd + 3, d.w);
+        rs[rt].x += d.x; rs[rt].y += d.y; rs[rt].z += d.z; rs[rt].w += d.w;
+    }
+    for (int q = 0; q < 5; ++q) {
+        float* gr = g_rate + (size_t)q * kEmb + 4 * lane;
+        atomicAdd(gr, rs[q].x); atomicAdd(gr + 1, rs[q].y); atomicAdd(gr + 2, rs[q].z); atomicAdd(gr + 3, rs[q].w);
+    }
+}
+
+// Standardised targets of a batch: [p_u (f), b_u, alpha_u].
+__global__ void k_targets(DeviceState s, const uint32_t* __restrict__ users, int n, int O,
+                          const float* __restrict__ mean, const float* __restrict__ inv_std, float* __restrict__ t) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * O) return;
+    const int r = e / O, c = e % O;
+    const uint32_t u = users[r];
+    float v;
+    if (c < (int)s.F) v = s.ufeat[(size_t)u * s.Fs + c];
+    else if (c == (int)s.F) v = s.ubias[u];
+    else v = s.alpha_u[u];
+    t[e] = (v - mean[c]) * inv_std[c];
+}
+
+// dY = 2 (y - t) / (n * O); per-block partial sums of the squared error.
+__global__ void k_mse(const float* __restrict__ y, const float* __restrict__ t, int total, float scale,
+                      float* __restrict__ dy, __nv_bfloat16* __restrict__ dyb, double* __restrict__ part) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const float d = y[e] - t[e];
+        acc += (double)d * d;
+        const float g = 2.0f * d * scale;
+        dy[e] = g;
+        dyb[e] = __float2bfloat16(g);
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// dZ = dH * GELU'(Z) -> BF16
+__global__ void k_gelu_bwd(const float* __restrict__ dh, const float* __restrict__ z, int total,
+                           __nv_bfloat16* __restrict__ dzb) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x)
+        dzb[e] = __float2bfloat16(dh[e] * gelu_grad(z[e]));
+}
+
+// column sums of a [rows, cols] matrix (bias gradients)
+__global__ void k_colsum_f(const float* __restrict__ x, int rows, int cols, float* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float a = 0.0f;
+    for (int r = 0; r < rows; ++r) a += x[(size_t)r * cols + c];
+    out[c] = a;
+}
+
+__global__ void k_colsum(const __nv_bfloat16* __restrict__ x, int rows, int cols, float* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float a = 0.0f;
+    for (int r = 0; r < rows; ++r) a += __bfloat162float(x[(size_t)r * cols + c]);
+    out[c] = a;
+}
+
+__global__ void k_adamw(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                        float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps, float wd, float c1,
+                        float c2, __nv_bfloat16* __restrict__ wb) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const float gg = g[e];
+        const float mm = b1 * m[e] + (1.0f - b1) * gg;
+        const float vv = b2 * v[e] + (1.0f - b2) * gg * gg;
+        m[e] = mm;
+        v[e] = vv;
+        const float upd = (mm / c1) / (sqrtf(vv / c2) + eps) + wd * w[e];
+        const float nw = w[e] - lr * upd;
+        w[e] = nw;
+        if (wb) wb[e] = __float2bfloat16(nw);
+    }
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ x, size_t n, __nv_bfloat16* __restrict__ y) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        y[e] = __float2bfloat16(x[e]);
+}
+
+// Writes de-standardised predictions into the model's user tables and resets
+// the rest of each user's state to the standard init (p2 = 0, but_bin = 0,
+// cu = 1, ubias_day = 0 on the user's days).
+__global__ void k_apply_users(DeviceState s, const uint32_t* __restrict__ users, int n, int O,
+                              const float* __restrict__ y, const float* __restrict__ mean,
+                              const float* __restrict__ std) {
+    const int w = blockIdx.x;
+    if (w >= n) return;
+    const uint32_t u = users[w];
+    for (uint32_t c = threadIdx.x; c < s.Fs; c += blockDim.x) {
+        s.ufeat[(size_t)u * s.Fs + c] = c < s.F ? y[(size_t)w * O + c] * std[c] + mean[c] : 0.0f;
+        s.ufeat2[(size_t)u * s.Fs + c] = 0.0f;
+    }
+    for (uint32_t b = threadIdx.x; b < s.T; b += blockDim.x) s.but_bin[(size_t)u * s.T + b] = 0.0f;
+    for (uint64_t d = s.ud_start[u] + threadIdx.x; d < s.ud_start[u + 1]; d += blockDim.x) s.ubias_day[d] = 0.0f;
+    if (threadIdx.x == 0) {
+        s.ubias[u] = y[(size_t)w * O + s.F] * std[s.F] + mean[s.F];
+        s.alpha_u[u] = y[(size_t)w * O + s.F + 1] * std[s.F + 1] + mean[s.F + 1];
+        s.cu[u] = 1.0f;
+    }
+}
+
+struct Param {
+    std::string name;
+    size_t n;
+    bool decay;
+    DevMem w, g, m, v, wb;  // wb only for GEMM weights
+};
+
+}  // namespace
+}  // namespace tsvd
+
+struct tsvd_encoder {
+    const tsvd_model* model = nullptr;
+    int O = 0;
+    float lr = 1e-3f, wd = 1e-4f, b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    uint64_t step = 0;
+    std::vector<tsvd::Param> params;  // e_item, e_rate, e_date, W1, b1, W2, b2, W3, b3
+    tsvd::DevMem raw, mean, inv_std, std_;
+    tsvd::DevMem users, h0, h0b, z1, h1b, z2, h2b, y, t, dy, dyb, dh2, dz2b, dh1, dz1b, dh0, part;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    double last_loss = 0.0;
+};
+
+namespace {
+
+thread_local std::string g_enc_err;
+
+tsvd::Param& P(tsvd_encoder* e, int k) { return e->params[k]; }
+
+template <class F>
+int eguard(tsvd_encoder* e, F&& f) {
+    try {
+        f();
+        return TSVD_OK;
+    } catch (const Error& x) {
+        if (e) e->err = x.what();
+        g_enc_err = x.what();
+        return x.status;
+    } catch (const std::exception& x) {
+        if (e) e->err = x.what();
+        g_enc_err = x.what();
+        return TSVD_ERR_INVALID;
+    }
+}
+
+unsigned grid_for(size_t n, unsigned block = 256) {
+    return (unsigned)std::min<size_t>((n + block - 1) / block, 148 * 32);
+}
+
+// forward over n users already in e->users; fills y (and activations)
+void forward(tsvd_encoder* e, int n) {
+    using namespace tsvd;
+    const DeviceState& s = e->model->d;
+    cudaStream_t st = e->stream;
+    k_embag_fwd<<<(n + 7) / 8, 256, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n,
+                                             P(e, 0).w.as<float>(), P(e, 1).w.as<float>(), P(e, 2).w.as<float>(),
+                                             e->h0.as<float>(), e->h0b.as<__nv_bfloat16>());
+    TSVD_CUDA(cudaGetLastError());
+    gemm(st, e->h0b.as<__nv_bfloat16>(), 0, kEmb, P(e, 3).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kEmb,
+         P(e, 4).w.as<float>(), e->z1.as<float>(), e->h1b.as<__nv_bfloat16>(), kHid, 1);
+    gemm(st, e->h1b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kHid,
+         P(e, 6).w.as<float>(), e->z2.as<float>(), e->h2b.as<__nv_bfloat16>(), kHid, 1);
+    gemm(st, e->h2b.as<__nv_bfloat16>(), 0, kHid, P(e, 7).wb.as<__nv_bfloat16>(), 1, e->O, n, e->O, kHid,
+         P(e, 8).w.as<float>(), e->y.as<float>(), nullptr, e->O, 0);
+}
+
+// loss and gradients for n users in e->users (targets from the model)
+double backward(tsvd_encoder* e, int n) {
+    using namespace tsvd;
+    const DeviceState& s = e->model->d;
+    cudaStream_t st = e->stream;
+    const int O = e->O;
+    k_targets<<<(n * O + 255) / 256, 256, 0, st>>>(s, e->users.as<uint32_t>(), n, O, e->mean.as<float>(),
+                                                   e->inv_std.as<float>(), e->t.as<float>());
+    const int nb = 256;
+    k_mse<<<nb, 256, 0, st>>>(e->y.as<float>(), e->t.as<float>(), n * O, 1.0f / ((float)n * O), e->dy.as<float>(),
+                              e->dyb.as<__nv_bfloat16>(), e->part.as<double>());
+    TSVD_CUDA(cudaGetLastError());
+    // layer 3
+    gemm(st, e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, O, kHid, O, n, nullptr,
+         P(e, 7).g.as<float>(), nullptr, O, 0);
+    k_colsum_f<<<(O + 127) / 128, 128, 0, st>>>(e->dy.as<float>(), n, O, P(e, 8).g.as<float>());
+    gemm(st, e->dyb.as<__nv_bfloat16>(), 0, O, P(e, 7).wb.as<__nv_bfloat16>(), 0, O, n, kHid, O, nullptr,
+         e->dh2.as<float>(), nullptr, kHid, 0);
+    k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh2.as<float>(), e->z2.as<float>(), n * kHid,
+                                                           e->dz2b.as<__nv_bfloat16>());
+    // layer 2
+    gemm(st, e->h1b.as<__nv_bfloat16>(), 1, kHid, e->dz2b.as<__nv_bfloat16>(), 1, kHid, kHid, kHid, n, nullptr,
+         P(e, 5).g.as<float>(), nullptr, kHid, 0);
+    k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz2b.as<__nv_bfloat16>(), n, kHid, P(e, 6).g.as<float>());
+    gemm(st, e->dz2b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 0, kHid, n, kHid, kHid, nullptr,
+         e->dh1.as<float>(), nullptr, kHid, 0);
+    k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh1.as<float>(), e->z1.as<float>(), n * kHid,
+                                                           e->dz1b.as<__nv_bfloat16>());
+    // layer 1
+    gemm(st, e->h0b.as<__nv_bfloat16>(), 1, kEmb, e->dz1b.as<__nv_bfloat16>(), 1, kHid, kEmb, kHid, n, nullptr,
+         P(e, 3).g.as<float>(), nullptr, kHid, 0);
+    k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz1b.as<__nv_bfloat16>(), n, kHid, P(e, 4).g.as<float>());
+    gemm(st, e->dz1b.as<__nv_bfloat16>(), 0, kHid, P(e, 3).wb.as<__nv_bfloat16>(), 0, kHid, n, kEmb, kHid, nullptr,
+         e->dh0.as<float>(), nullptr, kEmb, 0);
+    // embeddings
+    for (int k = 0; k < 3; ++k) TSVD_CUDA(cudaMemsetAsync(P(e, k).g.p, 0, P(e, k).n * 4, st));
+    k_embag_bwd<<<(n + 7) / 8, 256, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n, e->dh0.as<float>(),
+                                             P(e, 0).g.as<float>(), P(e, 1).g.as<float>(), P(e, 2).g.as<float>());
+    TSVD_CUDA(cudaGetLastError());
+    std::vector<double> part(nb);
+    TSVD_CUDA(cudaMemcpyAsync(part.data(), e->part.p, nb * 8, cudaMemcpyDeviceToHost, st));
+    TSVD_CUDA(cudaStreamSynchronize(st));
+    double sse = 0.0;
+    for (double v : part) sse += v;
+    return sse / ((double)n * O);
+}
+
+void adamw_step(tsvd_encoder* e) {
+    using namespace tsvd;
+    e->step++;
+    const float c1 = 1.0f - std::pow(e->b1, (float)e->step), c2 = 1.0f - std::pow(e->b2, (float)e->step);
+    for (auto& p : e->params)
+        k_adamw<<<grid_for(p.n), 256, 0, e->stream>>>(p.w.as<float>(), p.g.as<float>(), p.m.as<float>(),
+                                                      p.v.as<float>(), p.n, e->lr, e->b1, e->b2, e->eps,
+                                                      p.decay ? e->wd : 0.0f, c1, c2,
+                                                      p.wb.p ? p.wb.as<__nv_bfloat16>() : nullptr);
+    TSVD_CUDA(cudaGetLastError());
+}
+
+void set_users(tsvd_encoder* e, const uint32_t* users, int n) {
+    TSVD_CUDA(cudaMemcpyAsync(e->users.p, users, (size_t)n * 4, cudaMemcpyHostToDevice, e->stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint32_t* target_users,
+                        uint64_t n_target, uint64_t seed, float lr, float weight_decay, tsvd_encoder** out) {
+    if (!m || !out || !train_raw) return TSVD_ERR_INVALID;
+    *out = nullptr;
+    tsvd_encoder* e = new tsvd_encoder();
+    int rc = eguard(e, [&] {
+        using namespace tsvd;
+        TSVD_CUDA(cudaSetDevice(m->device));
+        e->model = m;
+        e->lr = lr;
+        e->wd = weight_decay;
+        const DeviceState& s = m->d;
+        e->O = (int)s.F + 2;
+        TSVD_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        e->raw.alloc(s.n_train);
+        TSVD_CUDA(cudaMemcpy(e->raw.p, train_raw, s.n_train, cudaMemcpyHostToDevice));
+        // parameters: Xavier-uniform matrices, N(0, 0.05) embeddings, zero biases
+        ChaCha12Stream g(seed);
+        auto add = [&](const char* name, size_t n, bool decay, bool bf16, float scale, bool uniform) {
+            Param p;
+            p.name = name;
+            p.n = n;
+            p.decay = decay;
+            std::vector<float> h(n, 0.0f);
+            if (scale > 0) {
+                for (size_t k = 0; k < n; ++k) {
+                    if (uniform) h[k] = scale * (2.0f * (float)(g.u32() >> 8) * (1.0f / 16777216.0f) - 1.0f);
+                    else h[k] = scale * (float)std_normal(g);
+                }
+            }
+            p.w.alloc(n * 4);
+            TSVD_CUDA(cudaMemcpy(p.w.p, h.data(), n * 4, cudaMemcpyHostToDevice));
+            p.g.alloc(n * 4);
+            p.m.alloc(n * 4);
+            p.v.alloc(n * 4);
+            TSVD_CUDA(cudaMemset(p.m.p, 0, n * 4));
+            TSVD_CUDA(cudaMemset(p.v.p, 0, n * 4));
+            if (bf16) {
+                p.wb.alloc(n * 2);
+                k_f32_to_bf16<<<grid_for(n), 256>>>(p.w.as<float>(), n, p.wb.as<__nv_bfloat16>());
+                TSVD_CUDA(cudaGetLastError());
+            }
+            e->params.push_back(std::move(p));
+        };
+        const int O = e->O;
+        add("e_item", (size_t)s.n_items * kEmb, false, false, 0.05f, false);
+        add("e_rate", 5 * kEmb, false, false, 0.05f, false);
+        add("e_date", (size_t)s.T * kEmb, false, false, 0.05f, false);
+        add("w1", (size_t)kEmb * kHid, true, true, std::sqrt(6.0f / (kEmb + kHid)), true);
+        add("b1", kHid, false, false, 0.0f, false);
+        add("w2", (size_t)kHid * kHid, true, true, std::sqrt(6.0f / (kHid + kHid)), true);
+        add("b2", kHid, false, false, 0.0f, false);
+        add("w3", (size_t)kHid * O, true, true, std::sqrt(6.0f / (kHid + O)), true);
+        add("b3", (size_t)O, false, false, 0.0f, false);
+        // target standardisation from the model's factors of the target users
+        std::vector<float> mean(O, 0.0f), sd(O, 1.0f);
+        if (target_users && n_target) {
+            std::vector<float> uf((size_t)s.n_users * s.F), ub(s.n_users), al(s.n_users);
+            TSVD_CUDA(cudaMemcpy2D(uf.data(), s.F * 4, s.ufeat, s.Fs * 4, s.F * 4, s.n_users, cudaMemcpyDeviceToHost));
+            TSVD_CUDA(cudaMemcpy(ub.data(), s.ubias, s.n_users * 4, cudaMemcpyDeviceToHost));
+            TSVD_CUDA(cudaMemcpy(al.data(), s.alpha_u, s.n_users * 4, cudaMemcpyDeviceToHost));
+            std::vector<double> s1(O, 0.0), s2(O, 0.0);
+            for (uint64_t k = 0; k < n_target; ++k) {
+                const uint32_t u = target_users[k];
+                if (u >= s.n_users) throw Error(TSVD_ERR_INVALID, "target user out of range");
+                for (int c = 0; c < O; ++c) {
+                    const double v = c < (int)s.F ? uf[(size_t)u * s.F + c] : (c == (int)s.F ? ub[u] : al[u]);
+                    s1[c] += v;
+                    s2[c] += v * v;
+                }
+            }
+            for (int c = 0; c < O; ++c) {
+                const double mu = s1[c] / n_target, var = std::max(s2[c] / n_target - mu * mu, 1e-20);
+                mean[c] = (float)mu;
+                sd[c] = (float)std::sqrt(var);
+            }
+        }
+        std::vector<float> inv(O);
+        for (int c = 0; c < O; ++c) inv[c] = 1.0f / sd[c];
+        e->mean.alloc(O * 4);
+        e->inv_std.alloc(O * 4);
+        e->std_.alloc(O * 4);
+        TSVD_CUDA(cudaMemcpy(e->mean.p, mean.data(), O * 4, cudaMemcpyHostToDevice));
+        TSVD_CUDA(cudaMemcpy(e->inv_std.p, inv.data(), O * 4, cudaMemcpyHostToDevice));
+        TSVD_CUDA(cudaMemcpy(e->std_.p, sd.data(), O * 4, cudaMemcpyHostToDevice));
+        // activations for kMaxBatch users
+        const size_t B = kMaxBatch;
+        e->users.alloc(B * 4);
+        e->h0.alloc(B * kEmb * 4);
+        e->h0b.alloc(B * kEmb * 2);
+        e->z1.alloc(B * kHid * 4);
+        e->h1b.alloc(B * kHid * 2);
+        e->z2.alloc(B * kHid * 4);
+        e->h2b.alloc(B * kHid * 2);
+        e->y.alloc(B * O * 4);
+        e->t.alloc(B * O * 4);
+        e->dy.alloc(B * O * 4);
+        e->dyb.alloc(B * O * 2);
+        e->dh2.alloc(B * kHid * 4);
+        e->dz2b.alloc(B * kHid * 2);
+        e->dh1.alloc(B * kHid * 4);
+        e->dz1b.alloc(B * kHid * 2);
+        e->dh0.alloc(B * kEmb * 4);
+        e->part.alloc(256 * 8);
+        TSVD_CUDA(cudaDeviceSynchronize());
+    });
+    if (rc != TSVD_OK) {
+        tsvd_encoder_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return TSVD_OK;
+}
+
+void tsvd_encoder_destroy(tsvd_encoder* e) {
+    if (!e) return;
+    if (e->stream) {
+        cudaStreamSynchronize(e->stream);
+        cudaStreamDestroy(e->stream);
+    }
+    delete e;
+}
+
+// One pass over `users` in mini-batches (batch <= 4096): forward, loss,
+// backward, AdamW. Returns the mean loss over the pass.
+int tsvd_encoder_train_epoch(tsvd_encoder* e, const uint32_t* users, uint64_t n, uint32_t batch, double* mean_loss) {
+    if (!e || !users) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(e->mu);
+    return eguard(e, [&] {
+        if (batch == 0 || batch > (uint32_t)tsvd::kMaxBatch) throw Error(TSVD_ERR_INVALID, "batch must be 1..4096");
+        TSVD_CUDA(cudaSetDevice(e->model->device));
+        double tot = 0.0;
+        uint64_t nb = 0;
+        for (uint64_t a = 0; a < n; a += batch) {
+            const int b = (int)std::min<uint64_t>(batch, n - a);
+            for (int k = 0; k < b; ++k)
+                if (users[a + k] >= e->model->d.n_users) throw Error(TSVD_ERR_INVALID, "user out of range");
+            set_users(e, users + a, b);
+            forward(e, b);
+            tot += backward(e, b);
+            adamw_step(e);
+            nb++;
+        }
+        TSVD_CUDA(cudaStreamSynchronize(e->stream));
+        e->last_loss = nb ? tot / nb : 0.0;
+        if (mean_loss) *mean_loss = e->last_loss;
+    });
+}
+
+// Loss and gradients for one batch without an update (for checking); the
+// gradients are read with tsvd_encoder_get("g.<name>").
+int tsvd_encoder_loss_grad(tsvd_encoder* e, const uint32_t* users, uint32_t n, double* loss) {
+    if (!e || !users) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(e->mu);
+    return eguard(e, [&] {
+        if (n == 0 || n > (uint32_t)tsvd::kMaxBatch) throw Error(TSVD_ERR_INVALID, "n must be 1..4096");
+        TSVD_CUDA(cudaSetDevice(e->model->device));
+        set_users(e, users, (int)n);
+        forward(e, (int)n);
+        const double l = backward(e, (int)n);
+        if (loss) *loss = l;
+    });
+}
+
+// Standardised outputs y [n, f+2] for `users` (host copy).
+int tsvd_encoder_forward(tsvd_encoder* e, const uint32_t* users, uint32_t n, float* out) {
+    if (!e || !users || !out) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(e->mu);
+    return eguard(e, [&] {
+        if (n == 0 || n > (uint32_t)tsvd::kMaxBatch) throw Error(TSVD_ERR_INVALID, "n must be 1..4096");
+        TSVD_CUDA(cudaSetDevice(e->model->device));
+        set_users(e, users, (int)n);
+        forward(e, (int)n);
+        TSVD_CUDA(cudaMemcpyAsync(out, e->y.p, (size_t)n * e->O * 4, cudaMemcpyDeviceToHost, e->stream));
+        TSVD_CUDA(cudaStreamSynchronize(e->stream));
+    });
+}
+
+// Writes the encoder's prediction of p_u, b_u, alpha_u into model m (which
+// may be e's model) for `users`; their other user state is reset to the
+// standard init.
+int tsvd_encoder_apply(tsvd_encoder* e, tsvd_model* m, const uint32_t* users, uint64_t n) {
+    if (!e || !m || !users) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(e->mu);
+    return eguard(e, [&] {
+        using namespace tsvd;
+        if (m->d.F != e->model->d.F || m->d.n_users != e->model->d.n_users)
+            throw Error(TSVD_ERR_INVALID, "model shape differs from the encoder's");
+        TSVD_CUDA(cudaSetDevice(e->model->device));
+        for (uint64_t a = 0; a < n; a += kMaxBatch) {
+            const int b = (int)std::min<uint64_t>(kMaxBatch, n - a);
+            for (int k = 0; k < b; ++k)
+                if (users[a + k] >= m->d.n_users) throw Error(TSVD_ERR_INVALID, "user out of range");
+            set_users(e, users + a, b);
+            forward(e, b);
+            k_apply_users<<<b, 128, 0, e->stream>>>(m->d, e->users.as<uint32_t>(), b, e->O, e->y.as<float>(),
+                                                    e->mean.as<float>(), e->std_.as<float>());
+            TSVD_CUDA(cudaGetLastError());
+        }
+        TSVD_CUDA(cudaStreamSynchronize(e->stream));
+    });
+}
+
+// Parameter (or gradient, "g.<name>") access: names e_item, e_rate, e_date,
+// w1, b1, w2, b2, w3, b3; FP32 row-major, matrices [in, out].
+int tsvd_encoder_get(const tsvd_encoder* ec, const char* name, float* dst, uint64_t count) {
+    tsvd_encoder* e = const_cast<tsvd_encoder*>(ec);
+    if (!e || !name || !dst) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(e->mu);
+    return eguard(e, [&] {
+        std::string n(name);
+        bool grad = n.rfind("g.", 0) == 0;
+        if (grad) n = n.substr(2);
+        for (auto& p : e->params)
+            if (p.name == n) {
+                if (count != p.n) throw Error(TSVD_ERR_INVALID, "count mismatch for " + n);
+                TSVD_CUDA(cudaMemcpy(dst, grad ? p.g.p : p.w.p, count * 4, cudaMemcpyDeviceToHost));
+                return;
+            }
+        throw Error(TSVD_ERR_INVALID, "unknown encoder parameter " + n);
+    });
+}
+
+int tsvd_encoder_set(tsvd_encoder* e, const char* name, const float* src, uint64_t count) {
+    if (!e || !name || !src) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(e->mu);
+    return eguard(e, [&] {
+        using namespace tsvd;
+        for (auto& p : e->params)
+            if (p.name == name) {
+                if (count != p.n) throw Error(TSVD_ERR_INVALID, "count mismatch");
+                TSVD_CUDA(cudaMemcpy(p.w.p, src, count * 4, cudaMemcpyHostToDevice));
+                if (p.wb.p) {
+                    k_f32_to_bf16<<<grid_for(p.n), 256, 0, e->stream>>>(p.w.as<float>(), p.n,
+                                                                       p.wb.as<__nv_bfloat16>());
+                    TSVD_CUDA(cudaStreamSynchronize(e->stream));
+                }
+                return;
+            }
+        throw Error(TSVD_ERR_INVALID, std::string("unknown encoder parameter ") + name);
+    });
+}
+
+// Standardisation used for the targets: mean[f+2], std[f+2].
+int tsvd_encoder_target_stats(const tsvd_encoder* ec, float* mean, float* std_out) {
+    tsvd_encoder* e = const_cast<tsvd_encoder*>(ec);
+    if (!e || !mean || !std_out) return TSVD_ERR_INVALID;
+    return eguard(e, [&] {
+        TSVD_CUDA(cudaMemcpy(mean, e->mean.p, e->O * 4, cudaMemcpyDeviceToHost));
+        TSVD_CUDA(cudaMemcpy(std_out, e->std_.p, e->O * 4, cudaMemcpyDeviceToHost));
+    });
+}
+
+const char* tsvd_encoder_last_error(const tsvd_encoder* e) { return e ? e->err.c_str() : g_enc_err.c_str(); }
+
+}  // extern "C"

@@ -13,26 +13,13 @@
 //              user stratum with frozen item tables (no conflicts), NSVD1
 //              deltas reduced per item in by-item order, ycache rebuild,
 //              item stratum with frozen user tables. Deterministic.
+#include <algorithm>
 #include <cstring>
 
 #include "rand_stream.hpp"
-#include "tsvd_device.cuh"
+#include "tsvd_epoch.cuh"
 
 namespace tsvd {
-namespace {
-
-constexpr int kWarps = 8;  // warps per block
-constexpr int kThreads = kWarps * 32;
-
-struct EpochParams {
-    float lr_u, lr_u2, lr_ub, lr_ubd, lr_i, lr_ib, lr_y, lr_yb, lr_tu, lr_ti, lr_ta, lr_ibf, lr_iqf, lr_cu;
-    float reg_iqf, reg_cu, reg_u, reg_u2, reg_i, reg_y;
-    float w_bias, w_factor;
-    float nsvd_norm_exp;
-    int32_t sum_err_bug;
-    int32_t full_su;
-    int32_t use_ycache;  // su of a user equals ycache[u] (stratified, full_su, ycache valid)
-};
 
 EpochParams make_params(const tsvd_model* m) {
     const tsvd_config& c = m->cfg;
@@ -47,72 +34,87 @@ EpochParams make_params(const tsvd_model* m) {
     p.sum_err_bug = c.sum_err_bug;
     p.full_su = c.full_su;
     p.use_ycache = 0;
+    p.stages = 4;
     return p;
 }
 
-// Sum of y rows (and ybias) over `n` items produced by `item_of(k)`, in order.
+namespace {
+
+// ---------------------------------------------------------------------------
+// Hogwild epoch, software-pipelined. The arithmetic is k_user_pass<VPL, true>'s
+// (the reference's per-user pass); what changes is when data is fetched, so a
+// warp stops waiting on memory between dependent ratings:
+//  - the q_i and q^f_{i,0} rows of the next ST - 1 ratings are staged in a
+//    per-warp shared-memory ring by cp.async, together with the item-bias
+//    scalars, cut and the rating's record fields;
+//  - ubias_day of the next ST - 1 ratings is prefetched into registers; when
+//    one of them is on the same (user, day) as the rating just updated, the
+//    prefetched value is replaced by the value just written, so every rating
+//    sees the reference's sequential value;
+//  - the su gather and the end-of-user y update keep 8 rows in flight.
+// ---------------------------------------------------------------------------
+constexpr int kStages = 4;  // default ring depth (the batched form tunes it per width)
+constexpr int kBatch = 8;
+
+// su += y_j for the items given by item_of(0..n-1), in order, 8 rows in flight.
 template <int VPL, class ItemOf>
-__device__ __forceinline__ void gather_y(const DeviceState& s, uint64_t n, ItemOf item_of, int lane, float (&su)[VPL],
-                                         float& sub) {
+__device__ __forceinline__ void gather_y8(const DeviceState& s, uint64_t n, ItemOf item_of, int lane,
+                                          float (&su)[VPL], float& sub) {
     for (uint64_t base = 0; base < n; base += 32) {
         const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
         const uint32_t mine = lane < (int)cnt ? item_of(base + lane) : 0u;
-#pragma unroll 4
-        for (uint32_t j = 0; j < cnt; ++j) {
-            const uint32_t it = __shfl_sync(kFull, mine, j);
-            float y[VPL];
-            Row<VPL>::load_cg(s.yfeat + (size_t)it * s.Fs, lane, y);
+        for (uint32_t j = 0; j < cnt; j += kBatch) {
+            float y[kBatch][VPL], yb[kBatch];
 #pragma unroll
-            for (int v = 0; v < VPL; ++v) su[v] += y[v];
-            sub += __ldcg(s.ybias + it);
+            for (int q = 0; q < kBatch; ++q) {
+                const uint32_t it = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
+                Row<VPL>::load_cg(s.yfeat + (size_t)it * s.Fs, lane, y[q]);
+                yb[q] = __ldcg(s.ybias + it);
+            }
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                if (j + q < cnt) {
+#pragma unroll
+                    for (int v = 0; v < VPL; ++v) su[v] += y[q][v];
+                    sub += yb[q];
+                }
+            }
         }
     }
 }
 
-// ---------------------------------------------------------------------------
-// User stratum (both schedules).
-// ---------------------------------------------------------------------------
-template <int VPL, bool HOG>
-__global__ void __launch_bounds__(kThreads) k_user_pass(DeviceState s, EpochParams p, const uint32_t* __restrict__ order,
-                                                        uint32_t n_work) {
-    const int lane = threadIdx.x & 31;
+// One user of a Hogwild epoch, by one warp; `ring` is the warp's
+// ST * (2 Fs + 8)-float shared-memory slice; ratings are staged ST - 1 ahead.
+template <int VPL, int ST = kStages>
+__device__ __forceinline__ void hog_user(const DeviceState& s, const EpochParams& p, uint32_t u, float* ring,
+                                         int lane) {
+    constexpr int AH = ST - 1;
     const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
-    (void)NF;
-    for (;;) {
-        uint32_t k = 0;
-        if (lane == 0) k = atomicAdd(&s.counters[0], 1u);
-        k = __shfl_sync(kFull, k, 0);
-        if (k >= n_work) break;
-        const uint32_t u = order[k];
+    const uint32_t slot_f = 2 * Fs + kSlotScalars;  // q row, q^f row, scalars
+    {
         const uint64_t start = s.user_off[u], end = s.user_off[u + 1];
-        if (start == end) continue;
-        const uint64_t ps = s.pr_off[u], pe = s.pr_off[u + 1];
-        const uint64_t total = (end - start) + (p.full_su ? (pe - ps) : 0);
+        if (start == end) return;
+        const uint64_t n = end - start;
+        const Rec* rr = s.rec + start;
+        const uint64_t ps = s.pr_off[u], pe_ = s.pr_off[u + 1];
+        const uint64_t total = n + (p.full_su ? (pe_ - ps) : 0);
         const float norm = sqrtf((float)total);
 
-        // ---- NSVD1 user sum su = |N(u)|^-1/2 sum_j y_j (src/tx.rs:800-822)
-        float su[VPL], sub;
-        if (!HOG && p.use_ycache) {
-            Row<VPL>::load_cg(s.ycache + (size_t)u * Fs, lane, su);
-            sub = __ldcg(s.ycache_bias + u);
-        } else {
+        // ---- su (src/tx.rs:800-822), from the current y
+        float su[VPL], sub = 0.0f;
 #pragma unroll
-            for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
-            sub = 0.0f;
-            const Rec* rr = s.rec + start;
-            gather_y<VPL>(s, end - start, [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sub);
-            if (p.full_su) {
-                const uint32_t* pp = s.pr_item + ps;
-                gather_y<VPL>(s, pe - ps, [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sub);
-            }
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) su[v] = su[v] / norm;
-            sub = sub / norm;
-            Row<VPL>::store(s.ycache + (size_t)u * Fs, lane, su);
-            if (lane == 0) s.ycache_bias[u] = sub;
+        for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
+        gather_y8<VPL>(s, n, [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sub);
+        if (p.full_su) {
+            const uint32_t* pp = s.pr_item + ps;
+            gather_y8<VPL>(s, pe_ - ps, [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sub);
         }
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) su[v] = su[v] / norm;
+        sub = sub / norm;
+        Row<VPL>::store(s.ycache + (size_t)u * Fs, lane, su);
+        if (lane == 0) s.ycache_bias[u] = sub;
 
-        // ---- user state in registers
         float pu[VPL], p2[VPL], seq[VPL];
         Row<VPL>::load_cg(s.ufeat + (size_t)u * Fs, lane, pu);
         Row<VPL>::load_cg(s.ufeat2 + (size_t)u * Fs, lane, p2);
@@ -124,102 +126,148 @@ __global__ void __launch_bounds__(kThreads) k_user_pass(DeviceState s, EpochPara
         float sum_err = 0.0f;
         const float gb = s.gbias;
 
-        for (uint64_t base = start; base < end; base += 32) {
-            const uint32_t cnt = (uint32_t)(end - base < 32 ? end - base : 32);
-            Rec mine{};
-            if (lane < (int)cnt) mine = load_rec(s.rec + base + lane);
-            // software pipeline: rows of rating j+1 are requested before rating j is used
-            float qn[VPL], qfn[VPL];
-            {
-                const Rec r0 = shfl_rec(mine, 0);
-                const uint32_t i0 = rec_id(r0.key);
-                if (HOG) {
-                    Row<VPL>::load_cg(s.ifeat + (size_t)i0 * Fs, lane, qn);
-                    Row<VPL>::load_cg(s.ifeat_freq + (size_t)i0 * NF * Fs, lane, qfn);
-                } else {
-                    Row<VPL>::load_nc(s.ifeat + (size_t)i0 * Fs, lane, qn);
-                    Row<VPL>::load_nc(s.ifeat_freq + (size_t)i0 * NF * Fs, lane, qfn);
-                }
-            }
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const Rec r = shfl_rec(mine, j);
-                const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
-                float q[VPL], qf[VPL];
+        // record window for the issuer: cur = [w, w+32), nxt = [w+32, w+64)
+        uint64_t w = 0;
+        Rec cur{}, nxt{};
+        if ((uint64_t)lane < n) cur = load_rec(rr + lane);
+        if (32 + (uint64_t)lane < n) nxt = load_rec(rr + 32 + lane);
+        // ubias_day pipeline (lane 0): values and (user, day) indices of ratings t..t+AH
+        float bq[AH + 1];
+        uint32_t dq[AH + 1];
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) { q[v] = qn[v]; qf[v] = qfn[v]; }
-                const Rec rn = shfl_rec(mine, j + 1 < cnt ? j + 1 : j);
-                if (j + 1 < cnt) {
-                    const uint32_t in = rec_id(rn.key);
-                    if (HOG) {
-                        Row<VPL>::load_cg(s.ifeat + (size_t)in * Fs, lane, qn);
-                        Row<VPL>::load_cg(s.ifeat_freq + (size_t)in * NF * Fs, lane, qfn);
-                    } else {
-                        Row<VPL>::load_nc(s.ifeat + (size_t)in * Fs, lane, qn);
-                        Row<VPL>::load_nc(s.ifeat_freq + (size_t)in * NF * Fs, lane, qfn);
-                    }
-                }
-                // low_memory: the frequency bin used in training is always 0 (src/tx.rs:834,873)
-                const float ib = HOG ? __ldcg(s.ibias + i) : __ldg(s.ibias + i);
-                const float bit = HOG ? __ldcg(s.bit_bin + (size_t)i * T + tb) : __ldg(s.bit_bin + (size_t)i * T + tb);
-                const float ibf = HOG ? __ldcg(s.ibias_freq + (size_t)i * NF) : __ldg(s.ibias_freq + (size_t)i * NF);
-                float bud = 0.0f;
-                const bool hud = r.ud < s.n_ud;
-                if (lane == 0 && hud) bud = s.ubias_day[r.ud];
-                bud = __shfl_sync(kFull, bud, 0);
-                const float ct = hud ? __ldg(s.cut + r.ud) : 0.0f;
-                const float but = __shfl_sync(kFull, tb < 32 ? bb0 : bb1, tb & 31);
-                const float dv = r.dev;
-                const float bu_t = ub + but + al * dv + bud + sub;
-                const float bi_t = ib + bit + ibf;
-                const float cu_t = cuu + ct;
-                float part = 0.0f;
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
-                const float dot = warp_sum(part);
-                const float score = gb + bu_t + bi_t * cu_t + dot;
-                const float err = score - r.res;
-                const float err_b = HOG ? err * p.w_bias : err;
-                const float err_d = HOG ? err * p.w_factor : err;
-
-                ub -= p.lr_ub * err_b;
-                {
-                    const float nb = but - p.lr_tu * err_b;
-                    if (lane == (int)(tb & 31)) {
-                        if (tb < 32) bb0 = nb;
-                        else bb1 = nb;
-                    }
-                }
-                al -= p.lr_ta * err_b * dv;
-                if (lane == 0 && hud) s.ubias_day[r.ud] = bud - p.lr_ubd * err_b;
-                if (HOG && lane == 0) {
-                    __stcg(s.ibias + i, ib - p.lr_ib * (err_b * cu_t));
-                    __stcg(s.bit_bin + (size_t)i * T + tb, bit - p.lr_ti * (err_b * cu_t));
-                    __stcg(s.ibias_freq + (size_t)i * NF, ibf - p.lr_ibf * (err_b * cu_t));
-                }
-                cuu -= p.lr_cu * (err_b * bi_t + p.reg_cu * (cuu - 1.0f));
-                if (!p.sum_err_bug) sum_err += err_b;
-                else
-                    for (uint32_t kk = 0; kk < s.F; ++kk) sum_err += err_b;
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) {
-                    const float qe = q[v] + qf[v];
-                    const float pk = pu[v], p2k = p2[v];
-                    seq[v] += err_d * qe;
-                    pu[v] = pk - p.lr_u * (err_d * qe + p.reg_u * pk);
-                    p2[v] = p2k - p.lr_u2 * (err_d * qe * dv + p.reg_u2 * p2k);
-                    if (HOG) {
-                        const float pe = pk + dv * p2k + 0.0f + su[v];
-                        q[v] = q[v] - p.lr_i * (err_d * pe + p.reg_i * q[v]);
-                        qf[v] = qf[v] - p.lr_iqf * (err_d * pe + p.reg_iqf * qf[v]);
-                    }
-                }
-                if (HOG) {
-                    Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
-                    Row<VPL>::store(s.ifeat_freq + (size_t)i * NF * Fs, lane, qf);
-                }
-            }
+        for (int a = 0; a <= AH; ++a) {
+            bq[a] = 0.0f;
+            dq[a] = 0xffffffffu;
         }
-        // ---- write back user state
+        auto shift = [&]() {
+#pragma unroll
+            for (int a = 0; a < AH; ++a) {
+                bq[a] = bq[a + 1];
+                dq[a] = dq[a + 1];
+            }
+        };
+
+        auto issue = [&](uint64_t t) {
+            if (t >= w + 64) {  // slide the window by one block
+                cur = nxt;
+                w += 32;
+                nxt = Rec{};
+                if (w + 32 + lane < n) nxt = load_rec(rr + w + 32 + lane);
+            }
+            float* slot = ring + (size_t)(t % ST) * slot_f;
+            if (t < n) {
+                const uint32_t o = (uint32_t)(t - w);
+                const Rec ra = shfl_rec(cur, o & 31), rb = shfl_rec(nxt, o & 31);
+                const Rec r = o < 32 ? ra : rb;
+                const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+                row_cp_async<VPL>(slot, s.ifeat + (size_t)i * Fs, lane);
+                row_cp_async<VPL>(slot + Fs, s.ifeat_freq + (size_t)i * NF * Fs, lane);
+                const bool hud = r.ud < s.n_ud;
+                float* sc = slot + 2 * Fs;
+                if (lane == 0) cp_async4(sc + 0, s.ibias + i);
+                if (lane == 1) cp_async4(sc + 1, s.bit_bin + (size_t)i * T + tb);
+                if (lane == 2) cp_async4(sc + 2, s.ibias_freq + (size_t)i * NF);
+                if (lane == 3) {
+                    if (hud) cp_async4(sc + 3, s.cut + r.ud);
+                    else sc[3] = 0.0f;
+                }
+                if (lane == 4) sc[4] = __uint_as_float(r.key);
+                if (lane == 5) sc[5] = r.res;
+                if (lane == 6) sc[6] = r.dev;
+                if (lane == 7) sc[7] = __uint_as_float(r.ud);
+                if (lane == 8) sc[8] = s.raw ? (float)__ldg(s.raw + (start + t)) : 0.0f;
+                float bnew = 0.0f;
+                if (lane == 0 && hud) bnew = s.ubias_day[r.ud];
+                bq[AH] = bnew;
+                dq[AH] = r.ud;
+            }
+            cp_async_commit();
+        };
+        // prologue: ratings 0..AH-1, shifted into the b/d pipeline
+        __syncwarp();  // the ring is reused from the previous user
+#pragma unroll
+        for (int a = 0; a < AH; ++a) {
+            issue((uint64_t)a);
+            shift();
+        }
+        for (uint64_t t = 0; t < n; ++t) {
+            __syncwarp();
+            issue(t + AH);
+            cp_async_wait<AH>();
+            __syncwarp();
+            const float* slot = ring + (size_t)(t % ST) * slot_f;
+            float q[VPL], qf[VPL];
+            row_from_smem<VPL>(slot, lane, q);
+            row_from_smem<VPL>(slot + Fs, lane, qf);
+            const float* sc = slot + 2 * Fs;
+            const float ib = sc[0], bit = sc[1], ibf = sc[2], ct = sc[3];
+            const uint32_t key = __float_as_uint(sc[4]);
+            const float res = sc[5], dv = sc[6];
+            const uint32_t ud = __float_as_uint(sc[7]);
+            const uint32_t i = rec_id(key), tb = rec_tbin(key);
+            const bool hud = ud < s.n_ud;
+            const float bud = __shfl_sync(kFull, bq[0], 0);
+            const float but = __shfl_sync(kFull, tb < 32 ? bb0 : bb1, tb & 31);
+            const float bu_t = ub + but + al * dv + bud + sub;
+            const float bi_t = ib + bit + ibf;
+            const float cu_t = cuu + ct;
+            float part = 0.0f;
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
+            const float dot = warp_sum(part);
+            const float score = gb + bu_t + bi_t * cu_t + dot;
+            // err = score - r, or the ordinal head's d(-log P)/d(score) (src/tx.rs:963-972)
+            float err = score - res;
+            if (s.raw) {  // thresholds are constant while lr_t = 0
+                const float th[4] = {__ldg(s.thresholds), __ldg(s.thresholds + 1), __ldg(s.thresholds + 2),
+                                     __ldg(s.thresholds + 3)};
+                err = ordinal_grad(th, score, (int)sc[8]);
+            }
+            const float err_b = err * p.w_bias, err_d = err * p.w_factor;
+            ub -= p.lr_ub * err_b;
+            {
+                const float nb = but - p.lr_tu * err_b;
+                if (lane == (int)(tb & 31)) {
+                    if (tb < 32) bb0 = nb;
+                    else bb1 = nb;
+                }
+            }
+            al -= p.lr_ta * err_b * dv;
+            if (lane == 0 && hud) {
+                const float nv = bud - p.lr_ubd * err_b;
+                s.ubias_day[ud] = nv;
+#pragma unroll
+                for (int a = 1; a <= AH; ++a)
+                    if (dq[a] == ud) bq[a] = nv;
+            }
+            if (lane == 0) {
+                // item-side updates are applied as atomic deltas: users that
+                // run concurrently never overwrite each other's update
+                atomicAdd(s.ibias + i, -(p.lr_ib * (err_b * cu_t)));
+                atomicAdd(s.bit_bin + (size_t)i * T + tb, -(p.lr_ti * (err_b * cu_t)));
+                atomicAdd(s.ibias_freq + (size_t)i * NF, -(p.lr_ibf * (err_b * cu_t)));
+            }
+            cuu -= p.lr_cu * (err_b * bi_t + p.reg_cu * (cuu - 1.0f));
+            if (!p.sum_err_bug) sum_err += err_b;
+            else
+                for (uint32_t kk = 0; kk < s.F; ++kk) sum_err += err_b;
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) {
+                const float qe = q[v] + qf[v];
+                const float pk = pu[v], p2k = p2[v];
+                seq[v] += err_d * qe;
+                pu[v] = pk - p.lr_u * (err_d * qe + p.reg_u * pk);
+                p2[v] = p2k - p.lr_u2 * (err_d * qe * dv + p.reg_u2 * p2k);
+                const float pe = pk + dv * p2k + 0.0f + su[v];
+                q[v] = -(p.lr_i * (err_d * pe + p.reg_i * q[v]));         // delta of q_i
+                qf[v] = -(p.lr_iqf * (err_d * pe + p.reg_iqf * qf[v]));   // delta of q^f_i
+            }
+            Row<VPL>::red_add(s.ifeat + (size_t)i * Fs, lane, q);
+            Row<VPL>::red_add(s.ifeat_freq + (size_t)i * NF * Fs, lane, qf);
+            shift();
+        }
+        cp_async_wait<0>();
+
         Row<VPL>::store(s.ufeat + (size_t)u * Fs, lane, pu);
         Row<VPL>::store(s.ufeat2 + (size_t)u * Fs, lane, p2);
         if (lane == 0) {
@@ -230,135 +278,184 @@ __global__ void __launch_bounds__(kThreads) k_user_pass(DeviceState s, EpochPara
         if (lane < (int)T) s.but_bin[(size_t)u * T + lane] = bb0;
         if (lane + 32 < (int)T) s.but_bin[(size_t)u * T + 32 + lane] = bb1;
 
-        if (HOG) {
-            // NSVD1 factor & bias updates at the end of the user (src/tx.rs:1099-1106)
-            float g[VPL];
+        // ---- NSVD1 factor & bias updates at the end of the user (src/tx.rs:1099-1106)
+        float g[VPL];
 #pragma unroll
-            for (int v = 0; v < VPL; ++v) g[v] = seq[v] / norm;
-            const float eb = sum_err / norm;
-            for (uint64_t base = start; base < end; base += 32) {
-                const uint32_t cnt = (uint32_t)(end - base < 32 ? end - base : 32);
-                const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&s.rec[base + lane].key)) : 0u;
-                for (uint32_t j = 0; j < cnt; ++j) {
-                    const uint32_t it = __shfl_sync(kFull, mine, j);
-                    float y[VPL];
-                    Row<VPL>::load_cg(s.yfeat + (size_t)it * Fs, lane, y);
+        for (int v = 0; v < VPL; ++v) g[v] = seq[v] / norm;
+        const float eb = sum_err / norm;
+        for (uint64_t base = 0; base < n; base += 32) {
+            const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
+            const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&rr[base + lane].key)) : 0u;
+            for (uint32_t j = 0; j < cnt; j += kBatch) {
+                float y[kBatch][VPL];
+                uint32_t its[kBatch];
 #pragma unroll
-                    for (int v = 0; v < VPL; ++v) y[v] = y[v] - p.lr_y * (g[v] + p.reg_y * y[v]);
-                    Row<VPL>::store(s.yfeat + (size_t)it * Fs, lane, y);
-                    if (lane == 0) __stcg(s.ybias + it, __ldcg(s.ybias + it) - p.lr_yb * eb);
-                }
-            }
-        } else {
-            float g[VPL];
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) g[v] = seq[v] / norm;
-            Row<VPL>::store(s.g_user + (size_t)u * Fs, lane, g);
-            if (lane == 0) s.e_user[u] = sum_err / norm;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Stratified: apply the NSVD1 deltas per item (apply_nsvd_deltas,
-// src/tsvdx4p.rs:341-385). The per-item sum over the item's users runs in two
-// fixed-order levels: fixed chunks of kChunkUsers consecutive by-item entries
-// are summed by one warp each (k_y_partial), then each item adds its chunk
-// partials in chunk order (k_y_combine). Same result on every run.
-// ---------------------------------------------------------------------------
-template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t Fs = s.Fs;
-    constexpr int B = 8;  // rows in flight per warp
-    for (;;) {
-        uint32_t c = 0;
-        if (lane == 0) c = atomicAdd(&s.counters[1], 1u);
-        c = __shfl_sync(kFull, c, 0);
-        if (c >= s.n_chunks) break;
-        const uint64_t a = s.chunk_lo[c];
-        uint64_t b = s.chunk_lo[c + 1];
-        if (b - a > kChunkUsers) b = a + kChunkUsers;
-        float acc[VPL];
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
-        float eacc = 0.0f;
-        for (uint64_t base = a; base < b; base += 32) {
-            const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
-            const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&s.irec[base + lane].key)) : 0u;
-            for (uint32_t j = 0; j < cnt; j += B) {
-                float g[B][VPL], e[B];
-#pragma unroll
-                for (int q = 0; q < B; ++q) {
-                    const uint32_t jj = j + q < cnt ? j + q : cnt - 1;
-                    const uint32_t u = __shfl_sync(kFull, mine, jj);
-                    Row<VPL>::load_nc(s.g_user + (size_t)u * Fs, lane, g[q]);
-                    e[q] = __ldg(s.e_user + u);
+                for (int q = 0; q < kBatch; ++q) {
+                    its[q] = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
+                    Row<VPL>::load_cg(s.yfeat + (size_t)its[q] * Fs, lane, y[q]);
                 }
 #pragma unroll
-                for (int q = 0; q < B; ++q) {
+                for (int q = 0; q < kBatch; ++q) {
                     if (j + q < cnt) {
 #pragma unroll
-                        for (int v = 0; v < VPL; ++v) acc[v] += g[q][v];
-                        eacc += e[q];
+                        for (int v = 0; v < VPL; ++v) y[q][v] = -(p.lr_y * (g[v] + p.reg_y * y[q][v]));
+                        Row<VPL>::red_add(s.yfeat + (size_t)its[q] * Fs, lane, y[q]);
+                        if (lane == 0) atomicAdd(s.ybias + its[q], -(p.lr_yb * eb));
                     }
                 }
             }
         }
-        Row<VPL>::store(s.chunk_part + (size_t)c * Fs, lane, acc);
-        if (lane == 0) s.chunk_epart[c] = eacc;
     }
 }
 
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochParams p) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t Fs = s.Fs;
-    const uint32_t warps = gridDim.x * kWarps;
-    for (uint32_t i = blockIdx.x * kWarps + (threadIdx.x >> 5); i < s.n_items; i += warps) {
-        const uint32_t c0 = s.item_chunk0[i], c1 = s.item_chunk0[i + 1];
-        if (c0 == c1) continue;
-        float acc[VPL];
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
-        float eacc = 0.0f;
-        for (uint32_t c = c0; c < c1; ++c) {
-            float g[VPL];
-            Row<VPL>::load_cg(s.chunk_part + (size_t)c * Fs, lane, g);
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) acc[v] += g[v];
-            eacc += __ldcg(s.chunk_epart + c);
-        }
-        const float nc = (float)(s.item_off[i + 1] - s.item_off[i]);
-        const float scale = p.nsvd_norm_exp == 0.0f ? 1.0f : powf(nc, p.nsvd_norm_exp);
-        float y[VPL];
-        Row<VPL>::load_cg(s.yfeat + (size_t)i * Fs, lane, y);
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) y[v] = y[v] - p.lr_y * (acc[v] / scale + p.reg_y * y[v]);
-        Row<VPL>::store(s.yfeat + (size_t)i * Fs, lane, y);
-        if (lane == 0) s.ybias[i] = s.ybias[i] - p.lr_yb * (eacc / scale);
+__global__ void __launch_bounds__(kThreads, 2) k_hog_pass(DeviceState s, EpochParams p,
+                                                          const uint32_t* __restrict__ order, uint32_t n_work) {
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* ring = smem + (size_t)warp * kStages * (2 * s.Fs + kSlotScalars);
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(&s.counters[0], 1u);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= n_work) break;
+        hog_user<VPL>(s, p, order[k], ring, lane);
     }
 }
+
+// Out-of-line entry for the batched kernel: each (VPL, ring depth) instance
+// keeps its own register allocation (the call costs once per user, not per
+// rating).
+template <int VPL, int ST>
+__device__ __noinline__ void hog_user_st(const DeviceState* s, const EpochParams* p, uint32_t u, float* ring,
+                                         int lane) {
+    hog_user<VPL, ST>(*s, *p, u, ring, lane);
+}
+
+template <int VPL>
+__device__ __forceinline__ void hog_user_call(const DeviceState* s, const EpochParams* p, uint32_t u, float* ring,
+                                              int lane) {
+    const int st = p->stages;
+    if (st == 2) hog_user_st<VPL, 2>(s, p, u, ring, lane);
+    else if (st == 3) hog_user_st<VPL, 3>(s, p, u, ring, lane);
+    else hog_user_st<VPL, 4>(s, p, u, ring, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Batched Hogwild epoch: several model variants over one dataset in a single
+// persistent launch. A work unit is (variant, user), packed as
+// variant << 24 | user; units of the same user for every variant are adjacent,
+// so a user's rating records are read while still in L2. Each unit runs the
+// variant's VPL instance of hog_user; the shared-memory ring is sized for the
+// widest variant.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 2) k_hog_batched(const DeviceState* __restrict__ states,
+                                                             const EpochParams* __restrict__ params,
+                                                             const uint32_t* __restrict__ units, uint32_t n_units,
+                                                             uint32_t ring_floats, uint32_t* __restrict__ counter) {
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* ring = smem + (size_t)warp * ring_floats;
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(counter, 1u);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= n_units) break;
+        const uint32_t unit = units[k];
+        const uint32_t mk = unit >> 24, u = unit & 0xffffffu;
+        const DeviceState* s = states + mk;
+        const EpochParams* p = params + mk;
+        switch (s->Fs >> 5) {
+            case 1: hog_user_call<1>(s, p, u, ring, lane); break;
+            case 2: hog_user_call<2>(s, p, u, ring, lane); break;
+            case 3: hog_user_call<3>(s, p, u, ring, lane); break;
+            case 4: hog_user_call<4>(s, p, u, ring, lane); break;
+            case 5: hog_user_call<5>(s, p, u, ring, lane); break;
+            case 6: hog_user_call<6>(s, p, u, ring, lane); break;
+            case 7: hog_user_call<7>(s, p, u, ring, lane); break;
+            default: hog_user_call<8>(s, p, u, ring, lane); break;
+        }
+    }
+}
+
 
 // ---------------------------------------------------------------------------
 // ycache[u] = |N(u)|^-1/2 sum over train and pr items (rebuild_ycache,
 // src/tx.rs:391-418): train items in rating order, then pr items in pr order.
 // ---------------------------------------------------------------------------
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s) {
+__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, const __nv_bfloat16* __restrict__ ybf);
+
+template <int VPL>
+__device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bfloat16* __restrict__ ybf, uint32_t u,
+                                             int lane);
+
+// Batched ycache rebuild over (variant, user) pairs, variant-major.
+__global__ void __launch_bounds__(kThreads) k_rebuild_batched(const DeviceState* __restrict__ states,
+                                                              uint32_t n_models, uint32_t n_users) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * kWarps;
+    const uint64_t total = (uint64_t)n_models * n_users;
+    for (uint64_t w = blockIdx.x * (uint64_t)kWarps + (threadIdx.x >> 5); w < total; w += warps) {
+        const uint32_t mk = (uint32_t)(w / n_users), u = (uint32_t)(w - (uint64_t)mk * n_users);
+        const DeviceState& s = states[mk];
+        switch (s.Fs >> 5) {
+            case 1: rebuild_user<1>(s, nullptr, u, lane); break;
+            case 2: rebuild_user<2>(s, nullptr, u, lane); break;
+            case 3: rebuild_user<3>(s, nullptr, u, lane); break;
+            case 4: rebuild_user<4>(s, nullptr, u, lane); break;
+            case 5: rebuild_user<5>(s, nullptr, u, lane); break;
+            case 6: rebuild_user<6>(s, nullptr, u, lane); break;
+            case 7: rebuild_user<7>(s, nullptr, u, lane); break;
+            default: rebuild_user<8>(s, nullptr, u, lane); break;
+        }
+    }
+}
+
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, const __nv_bfloat16* __restrict__ ybf) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * kWarps;
-    for (uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5); u < s.n_users; u += warps) {
+    for (uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5); u < s.n_users; u += warps)
+        rebuild_user<VPL>(s, ybf, u, lane);
+}
+
+template <int VPL>
+__device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bfloat16* __restrict__ ybf, uint32_t u,
+                                             int lane) {
+    constexpr int B = 8;  // rows in flight
+    {
         float su[VPL];
 #pragma unroll
         for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
         float sub = 0.0f;
         const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
         const uint64_t pa = s.pr_off[u], pb = s.pr_off[u + 1];
-        const Rec* rr = s.rec + a;
-        gather_y<VPL>(s, b - a, [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sub);
-        const uint32_t* pp = s.pr_item + pa;
-        gather_y<VPL>(s, pb - pa, [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sub);
+        const uint64_t ntr = b - a, n = ntr + (pb - pa);
+        for (uint64_t base = 0; base < n; base += 32) {
+            const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
+            const uint64_t q = base + lane;
+            uint32_t mine = 0;
+            if (lane < (int)cnt) mine = q < ntr ? rec_id(__ldg(&s.rec[a + q].key)) : __ldg(s.pr_item + pa + (q - ntr));
+            for (uint32_t j = 0; j < cnt; j += B) {
+                float y[B][VPL], yb[B];
+#pragma unroll
+                for (int t = 0; t < B; ++t) {
+                    const uint32_t it = __shfl_sync(kFull, mine, j + t < cnt ? j + t : cnt - 1);
+                    if (ybf) row_load_bf16<VPL>(ybf + (size_t)it * s.Fs, lane, y[t]);
+                    else Row<VPL>::load_nc(s.yfeat + (size_t)it * s.Fs, lane, y[t]);
+                    yb[t] = __ldg(s.ybias + it);
+                }
+#pragma unroll
+                for (int t = 0; t < B; ++t) {
+                    if (j + t < cnt) {
+#pragma unroll
+                        for (int v = 0; v < VPL; ++v) su[v] += y[t][v];
+                        sub += yb[t];
+                    }
+                }
+            }
+        }
         const int32_t cnt = s.user_cnt_tr[u] + s.user_cnt_pr[u];
         if (cnt > 0) {
             const float nrm = sqrtf((float)cnt);
@@ -372,309 +469,44 @@ __global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s) {
 }
 
 // ---------------------------------------------------------------------------
-// Stratified item stratum (fit_epoch_item, src/tsvdx4p.rs:644-762): items in
-// parallel, each item's ratings in by-item order with the user tables frozen.
-//
-// An item's ratings form a serial chain (every update feeds the next dot
-// product), and the most-rated items carry ~0.5% of all ratings each, so the
-// chain of the hottest item bounds the pass. Items with >= kHeavy ratings get a
-// whole CTA, warp-specialised: warps 1..7 gather the user rows of the next
-// round of kRound ratings from HBM and fold them into
-// pe = (p_u + ycache_u) + dev * p2_u plus the rating's bias scalars in shared
-// memory (double-buffered rounds, one __syncthreads per round), while warp 0
-// runs the chain from shared memory only. Lighter items take one warp each,
-// with the next rating's rows prefetched into registers.
-// ---------------------------------------------------------------------------
-constexpr uint32_t kHeavy = 1024;
-constexpr int kRound = 32;  // ratings per buffered round
-
-struct ItemState {
-    float ib, bt0, bt1, bf0, bf1;
-};
-
-__device__ __forceinline__ ItemState load_item_state(const DeviceState& s, uint32_t i, int lane) {
-    const uint32_t T = s.T, NF = s.NF;
-    ItemState st;
-    st.ib = s.ibias[i];
-    st.bt0 = lane < (int)T ? s.bit_bin[(size_t)i * T + lane] : 0.0f;
-    st.bt1 = lane + 32 < (int)T ? s.bit_bin[(size_t)i * T + 32 + lane] : 0.0f;
-    st.bf0 = lane < (int)NF ? s.ibias_freq[(size_t)i * NF + lane] : 0.0f;
-    st.bf1 = lane + 32 < (int)NF ? s.ibias_freq[(size_t)i * NF + 32 + lane] : 0.0f;
-    return st;
-}
-
-__device__ __forceinline__ void store_item_state(const DeviceState& s, uint32_t i, int lane, const ItemState& st) {
-    const uint32_t T = s.T, NF = s.NF;
-    if (lane == 0) s.ibias[i] = st.ib;
-    if (lane < (int)T) s.bit_bin[(size_t)i * T + lane] = st.bt0;
-    if (lane + 32 < (int)T) s.bit_bin[(size_t)i * T + 32 + lane] = st.bt1;
-    if (lane < (int)NF) s.ibias_freq[(size_t)i * NF + lane] = st.bf0;
-    if (lane + 32 < (int)NF) s.ibias_freq[(size_t)i * NF + 32 + lane] = st.bf1;
-}
-
-// User-side scalars of one by-item rating: bu_t and cu_t (src/tsvdx4p.rs:690-708).
-__device__ __forceinline__ void user_scalars(const DeviceState& s, const Rec& r, float& bu_t, float& cu_t) {
-    const uint32_t u = rec_id(r.key), tb = rec_tbin(r.key);
-    const bool hud = r.ud < s.n_ud;
-    bu_t = __ldg(s.ubias + u) + __ldg(s.but_bin + (size_t)u * s.T + tb) + __ldg(s.alpha_u + u) * r.dev +
-           (hud ? __ldg(s.ubias_day + r.ud) : 0.0f) + __ldg(s.ycache_bias + u);
-    cu_t = __ldg(s.cu + u) + (hud ? __ldg(s.cut + r.ud) : 0.0f);
-}
-
-// One SGD step of the item chain; qf_at(v) is this lane's v-th element of q^f[fb].
-template <int VPL, class QF>
-__device__ __forceinline__ void item_step(const EpochParams& p, float gb, float (&q)[VPL], QF&& qf_at,
-                                          const float (&pe)[VPL], float bu_t, float cu_t, float res, uint32_t tb,
-                                          uint32_t fb, int lane, ItemState& st) {
-    const float bit = __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31);
-    const float ibf = __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
-    const float bi_t = st.ib + bit + ibf;
-    float qfv[VPL], part = 0.0f;
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-        qfv[v] = qf_at(v);
-        part += pe[v] * (q[v] + qfv[v]);
-    }
-    const float dot = warp_sum(part);
-    const float err = (gb + bu_t + bi_t * cu_t + dot) - res;
-    const float ec = err * cu_t;
-    st.ib -= p.lr_ib * ec;
-    const float nb = bit - p.lr_ti * ec;
-    if (lane == (int)(tb & 31)) {
-        if (tb < 32) st.bt0 = nb;
-        else st.bt1 = nb;
-    }
-    const float nf = ibf - p.lr_ibf * ec;
-    if (lane == (int)(fb & 31)) {
-        if (fb < 32) st.bf0 = nf;
-        else st.bf1 = nf;
-    }
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-        const float qi = q[v];
-        q[v] = qi - p.lr_i * (err * pe[v] + p.reg_i * qi);
-        qfv[v] = qfv[v] - p.lr_iqf * (err * pe[v] + p.reg_iqf * qfv[v]);
-    }
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) qf_at(v) = qfv[v];
-}
-
-template <int VPL>
-__device__ void item_light(const DeviceState& s, const EpochParams& p, uint32_t i, int lane) {
-    const uint32_t Fs = s.Fs, NF = s.NF;
-    const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
-    if (a == b) return;
-    float q[VPL];
-    Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
-    ItemState st = load_item_state(s, i, lane);
-    float* qf_base = s.ifeat_freq + (size_t)i * NF * Fs;
-    const float gb = s.gbias;
-    for (uint64_t base = a; base < b; base += 32) {
-        const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
-        Rec mine{};
-        if (lane < (int)cnt) mine = load_rec(s.irec + base + lane);
-        float pn[VPL], p2n[VPL], ycn[VPL];
-        {
-            const uint32_t u0 = rec_id(__shfl_sync(kFull, mine.key, 0));
-            Row<VPL>::load_nc(s.ufeat + (size_t)u0 * Fs, lane, pn);
-            Row<VPL>::load_nc(s.ufeat2 + (size_t)u0 * Fs, lane, p2n);
-            Row<VPL>::load_nc(s.ycache + (size_t)u0 * Fs, lane, ycn);
-        }
-        for (uint32_t j = 0; j < cnt; ++j) {
-            const Rec r = shfl_rec(mine, j);
-            float pe[VPL];
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) pe[v] = (pn[v] + ycn[v]) + r.dev * p2n[v];
-            if (j + 1 < cnt) {
-                const uint32_t un = rec_id(__shfl_sync(kFull, mine.key, j + 1));
-                Row<VPL>::load_nc(s.ufeat + (size_t)un * Fs, lane, pn);
-                Row<VPL>::load_nc(s.ufeat2 + (size_t)un * Fs, lane, p2n);
-                Row<VPL>::load_nc(s.ycache + (size_t)un * Fs, lane, ycn);
-            }
-            float bu_t, cu_t;
-            user_scalars(s, r, bu_t, cu_t);
-            const uint32_t tb = rec_tbin(r.key), fb = rec_fbin(r.key);
-            float* qrow = qf_base + (size_t)fb * Fs;
-            float qfv[VPL];
-            Row<VPL>::load_cg(qrow, lane, qfv);
-            item_step<VPL>(p, gb, q, [&](int v) -> float& { return qfv[v]; }, pe, bu_t, cu_t, r.res, tb, fb, lane,
-                           st);
-            Row<VPL>::store(qrow, lane, qfv);
-        }
-    }
-    Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
-    store_item_state(s, i, lane, st);
-}
-
-template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_item_pass(DeviceState s, EpochParams p) {
-    extern __shared__ float smem[];
-    __shared__ uint32_t sh_k;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t Fs = s.Fs, NF = s.NF;
-    const uint32_t stride = Fs + 4;  // one staged rating: pe row + {bu_t, cu_t, res, key}
-    float* qfs = smem;                                   // [NF][Fs]
-    float* buf = smem + (size_t)NF * Fs;                 // [2][kRound][stride]
-    for (;;) {
-        if (threadIdx.x == 0) sh_k = atomicAdd(&s.counters[2], 1u);
-        __syncthreads();
-        const uint32_t k = sh_k;
-        __syncthreads();
-        if (k >= s.n_items) return;
-        const uint32_t i = s.item_work[k];
-        const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
-        if (b - a < kHeavy) {
-            // Items are ordered heaviest first: from here on every item is light.
-            if (warp == 0) item_light<VPL>(s, p, i, lane);
-            for (;;) {
-                uint32_t k2 = 0;
-                if (lane == 0) k2 = atomicAdd(&s.counters[2], 1u);
-                k2 = __shfl_sync(kFull, k2, 0);
-                if (k2 >= s.n_items) return;
-                item_light<VPL>(s, p, s.item_work[k2], lane);
-            }
-        }
-        // ---------------- heavy item: whole CTA ----------------
-        for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
-            qfs[e] = __ldcg(s.ifeat_freq + (size_t)i * NF * Fs + e);
-        const uint64_t n = b - a;
-        const uint32_t rounds = (uint32_t)((n + kRound - 1) / kRound);
-        float q[VPL];
-        ItemState st{};
-        if (warp == 0) {
-            Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
-            st = load_item_state(s, i, lane);
-        }
-        // producers fill round r into buffer r & 1
-        auto produce = [&](uint32_t r) {
-            float* dst = buf + (size_t)(r & 1) * kRound * stride;
-            const uint64_t r0 = a + (uint64_t)r * kRound;
-            const uint64_t left = n - (uint64_t)r * kRound;
-            const uint32_t m = (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
-            for (uint32_t j = warp - 1; j < m; j += kWarps - 1) {
-                const Rec rr = load_rec(s.irec + r0 + j);
-                const uint32_t u = rec_id(rr.key);
-                float pu[VPL], p2[VPL], yc[VPL], pe[VPL];
-                Row<VPL>::load_nc(s.ufeat + (size_t)u * Fs, lane, pu);
-                Row<VPL>::load_nc(s.ufeat2 + (size_t)u * Fs, lane, p2);
-                Row<VPL>::load_nc(s.ycache + (size_t)u * Fs, lane, yc);
-                float bu_t, cu_t;
-                user_scalars(s, rr, bu_t, cu_t);
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) pe[v] = (pu[v] + yc[v]) + rr.dev * p2[v];
-                float* row = dst + (size_t)j * stride;
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) row[Row<VPL>::elem(lane, v)] = pe[v];
-                if (lane == 0) {
-                    row[Fs] = bu_t;
-                    row[Fs + 1] = cu_t;
-                    row[Fs + 2] = rr.res;
-                    row[Fs + 3] = __uint_as_float(rr.key);
-                }
-            }
-        };
-        if (warp > 0) produce(0);
-        __syncthreads();
-        const float gb = s.gbias;
-        for (uint32_t r = 0; r < rounds; ++r) {
-            if (warp > 0) {
-                if (r + 1 < rounds) produce(r + 1);
-            } else {
-                const float* src = buf + (size_t)(r & 1) * kRound * stride;
-                const uint64_t left = n - (uint64_t)r * kRound;
-                const uint32_t m = (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
-                for (uint32_t j = 0; j < m; ++j) {
-                    const float* row = src + (size_t)j * stride;
-                    float pe[VPL];
-#pragma unroll
-                    for (int v = 0; v < VPL; ++v) pe[v] = row[Row<VPL>::elem(lane, v)];
-                    const float bu_t = row[Fs], cu_t = row[Fs + 1], res = row[Fs + 2];
-                    const uint32_t key = __float_as_uint(row[Fs + 3]);
-                    const uint32_t tb = rec_tbin(key), fb = rec_fbin(key);
-                    float* qrow = qfs + (size_t)fb * Fs;
-                    item_step<VPL>(p, gb, q, [&](int v) -> float& { return qrow[Row<VPL>::elem(lane, v)]; }, pe,
-                                   bu_t, cu_t, res, tb, fb, lane, st);
-                }
-            }
-            __syncthreads();
-        }
-        if (warp == 0) {
-            Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
-            store_item_state(s, i, lane, st);
-        }
-        for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
-            __stcg(s.ifeat_freq + (size_t)i * NF * Fs + e, qfs[e]);
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
-template <class K>
-unsigned persistent_grid(K kernel, size_t smem) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
-    if (per_sm < 1) per_sm = 1;
-    return (unsigned)(sms * per_sm);
-}
-
 template <int VPL>
-void launch_user_pass(tsvd_model* m, const EpochParams& p, const uint32_t* order, bool hog) {
-    if (hog) {
-        unsigned g = persistent_grid(k_user_pass<VPL, true>, 0);
-        k_user_pass<VPL, true><<<g, kThreads, 0, m->stream>>>(m->d, p, order, m->d.n_users);
-    } else {
-        unsigned g = persistent_grid(k_user_pass<VPL, false>, 0);
-        k_user_pass<VPL, false><<<g, kThreads, 0, m->stream>>>(m->d, p, order, m->d.n_users);
-    }
+void launch_hog_pass(tsvd_model* m, const EpochParams& p, const uint32_t* order) {
+    const size_t smem = (size_t)kWarps * kStages * (2 * m->d.Fs + kSlotScalars) * sizeof(float);
+    TSVD_CUDA(cudaFuncSetAttribute(k_hog_pass<VPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    unsigned g = persistent_grid(k_hog_pass<VPL>, smem);
+    k_hog_pass<VPL><<<g, kThreads, smem, m->stream>>>(m->d, p, order, m->d.n_users);
     TSVD_CUDA(cudaGetLastError());
     m->launches++;
 }
 
 template <int VPL>
-void launch_y_apply(tsvd_model* m, const EpochParams& p) {
-    unsigned g = persistent_grid(k_y_partial<VPL>, 0);
-    k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(m->d);
-    TSVD_CUDA(cudaGetLastError());
-    unsigned g2 = ceil_div(m->d.n_items, kWarps);
-    k_y_combine<VPL><<<g2, kThreads, 0, m->stream>>>(m->d, p);
-    TSVD_CUDA(cudaGetLastError());
-    m->launches += 2;
-}
-
-template <int VPL>
-void launch_rebuild(tsvd_model* m) {
+void launch_rebuild(tsvd_model* m, const __nv_bfloat16* ybf) {
     unsigned g = persistent_grid(k_rebuild_ycache<VPL>, 0);
-    k_rebuild_ycache<VPL><<<g, kThreads, 0, m->stream>>>(m->d);
+    k_rebuild_ycache<VPL><<<g, kThreads, 0, m->stream>>>(m->d, ybf);
     TSVD_CUDA(cudaGetLastError());
     m->launches++;
 }
 
-template <int VPL>
-void launch_item_pass(tsvd_model* m, const EpochParams& p) {
-    size_t smem = ((size_t)m->d.NF * m->d.Fs + 2ull * kRound * (m->d.Fs + 4)) * sizeof(float);
-    TSVD_CUDA(cudaFuncSetAttribute(k_item_pass<VPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    unsigned g = persistent_grid(k_item_pass<VPL>, smem);
-    k_item_pass<VPL><<<g, kThreads, smem, m->stream>>>(m->d, p);
+}  // namespace
+
+void launch_hog_batched(cudaStream_t st, const DeviceState* d_states, const EpochParams* d_params,
+                        const uint32_t* d_units, uint32_t n_units, uint32_t ring_floats, uint32_t* d_counter) {
+    const size_t smem = (size_t)kWarps * ring_floats * sizeof(float);
+    TSVD_CUDA(cudaFuncSetAttribute(k_hog_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    unsigned g = persistent_grid(k_hog_batched, smem);
+    k_hog_batched<<<g, kThreads, smem, st>>>(d_states, d_params, d_units, n_units, ring_floats, d_counter);
     TSVD_CUDA(cudaGetLastError());
-    m->launches++;
 }
 
-#define TSVD_DISPATCH(VPLV, CALL)                                              \
-    switch (VPLV) {                                                            \
-        case 1: { constexpr int V = 1; CALL; } break;                          \
-        case 2: { constexpr int V = 2; CALL; } break;                          \
-        case 3: { constexpr int V = 3; CALL; } break;                          \
-        case 4: { constexpr int V = 4; CALL; } break;                          \
-        case 5: { constexpr int V = 5; CALL; } break;                          \
-        case 6: { constexpr int V = 6; CALL; } break;                          \
-        case 7: { constexpr int V = 7; CALL; } break;                          \
-        case 8: { constexpr int V = 8; CALL; } break;                          \
-        default: throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256");       \
-    }
+void launch_rebuild_batched(cudaStream_t st, const DeviceState* d_states, uint32_t n_models, uint32_t n_users) {
+    unsigned g = persistent_grid(k_rebuild_batched, 0);
+    k_rebuild_batched<<<g, kThreads, 0, st>>>(d_states, n_models, n_users);
+    TSVD_CUDA(cudaGetLastError());
+}
+
+namespace {
 
 void reset_counters(tsvd_model* m) {
     TSVD_CUDA(cudaMemsetAsync(m->d.counters, 0, 64, m->stream));
@@ -682,10 +514,22 @@ void reset_counters(tsvd_model* m) {
 
 }  // namespace
 
+// Rebuild from the FP32 masters (explicit calls, Hogwild epochs).
 void rebuild_ycache(tsvd_model* m) {
     ProfScope ps(m, "rebuild_ycache");
     const int vpl = (int)(m->d.Fs / 32);
-    TSVD_DISPATCH(vpl, launch_rebuild<V>(m));
+    TSVD_DISPATCH(vpl, launch_rebuild<V>(m, nullptr));
+    m->ycache_valid = true;
+}
+
+// Rebuild inside a stratified epoch: from the BF16 read copy of y in the
+// precision form, else from the FP32 master.
+void launch_rebuild_ycache(tsvd_model* m) {
+    ProfScope ps(m, "rebuild_ycache");
+    const __nv_bfloat16* ybf =
+        m->opts.precision >= TSVD_PREC_BF16_READ ? m->m_bf_yfeat.as<__nv_bfloat16>() : nullptr;
+    const int vpl = (int)(m->d.Fs / 32);
+    TSVD_DISPATCH(vpl, launch_rebuild<V>(m, ybf));
     m->ycache_valid = true;
 }
 
@@ -708,24 +552,24 @@ void run_epoch(tsvd_model* m, uint64_t epoch) {
         TSVD_CUDA(cudaStreamSynchronize(m->stream));  // `order` leaves scope
         {
             ProfScope ps(m, "user_pass_hogwild");
-            TSVD_DISPATCH(vpl, launch_user_pass<V>(m, p, m->m_perm.as<uint32_t>(), true));
+            TSVD_DISPATCH(vpl, launch_hog_pass<V>(m, p, m->m_perm.as<uint32_t>()));
         }
         rebuild_ycache(m);
     } else {
         p.use_ycache = (c.full_su && m->ycache_valid) ? 1 : 0;
-        {
-            ProfScope ps(m, "user_pass_stratified");
-            TSVD_DISPATCH(vpl, launch_user_pass<V>(m, p, m->d.user_work, false));
+        stratified_epoch(m, p);
+    }
+    if (c.has_ordinal_head) {
+        // OrdinalHead::enforce_sorted_with_gap at the end of the epoch
+        // (src/tx.rs:1112-1114, src/lib.rs:518-525)
+        float* th = m->h_thresholds;
+        std::sort(th, th + 4);
+        for (int k = 1; k < 4; ++k) {
+            const float min_ok = th[k - 1] + c.ordinal_head.th_gap;
+            if (th[k] < min_ok) th[k] = min_ok;
         }
-        {
-            ProfScope ps(m, "y_apply");
-            TSVD_DISPATCH(vpl, launch_y_apply<V>(m, p));
-        }
-        rebuild_ycache(m);
-        {
-            ProfScope ps(m, "item_pass");
-            TSVD_DISPATCH(vpl, launch_item_pass<V>(m, p));
-        }
+        TSVD_CUDA(cudaMemcpyAsync(m->d.thresholds, th, 16, cudaMemcpyHostToDevice, m->stream));
+        TSVD_CUDA(cudaStreamSynchronize(m->stream));
     }
 }
 

@@ -37,6 +37,20 @@ struct DevMem {
     DevMem() = default;
     DevMem(const DevMem&) = delete;
     DevMem& operator=(const DevMem&) = delete;
+    DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevMem& operator=(DevMem&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
     ~DevMem() { release(); }
     void alloc(size_t b) {
         release();
@@ -127,6 +141,8 @@ struct tsvd_model {
 
     tsvd::DeviceState d{};
     bool ycache_valid = false;  // ycache equals a rebuild from the current yfeat
+    int stages = 4;             // Hogwild prefetch ring depth when run in a group
+    float h_thresholds[4] = {0, 0, 0, 0};  // ordinal head (host copy)
     uint64_t launches = 0;
 
     // device allocations
@@ -136,6 +152,8 @@ struct tsvd_model {
     tsvd::DevMem m_alpha_u, m_but_bin, m_bit_bin, m_ybias, m_ycache_bias;
     tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
     tsvd::DevMem m_g_user, m_e_user, m_user_work, m_item_work, m_counters;
+    // BF16 read copies (precision form)
+    tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_ufeat, m_bf_ufeat2, m_bf_ycache;
     tsvd::DevMem m_chunk_lo, m_item_chunk0, m_chunk_part, m_chunk_epart;
     tsvd::DevMem m_perm;          // [U] epoch order upload buffer
     tsvd::DevMem m_scratch;       // predict / rmse scratch
@@ -154,6 +172,7 @@ namespace tsvd {
 
 // setup (tsvd_setup.cu)
 void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_view& pr);
+void setup_params(tsvd_model* m);
 // epoch drivers (tsvd_epoch.cu)
 void run_epoch(tsvd_model* m, uint64_t epoch);
 void rebuild_ycache(tsvd_model* m);

@@ -3,6 +3,9 @@
 // behind calc_rmse (src/lib.rs:659-672). One warp per row; the SSE is reduced
 // in a fixed order (per-warp sums, per-block tree, then one block over the
 // block partials), so repeated calls are bitwise identical.
+#include <mutex>
+#include <string>
+
 #include "tsvd_device.cuh"
 
 namespace tsvd {
@@ -14,7 +17,14 @@ constexpr unsigned kSseBlocks = 148 * 4;
 struct PredParams {
     float beta;
     int32_t low_memory;
+    int32_t ordinal;  // apply the ordinal head: E[r] from the cumulative logits
 };
+
+// predict (src/tx.rs:713-724): score, or E[r] under the ordinal head
+__device__ __forceinline__ float finish_score(const DeviceState& s, const PredParams& pp, float bp, float dot) {
+    const float score = bp + dot + 0.0f;
+    return pp.ordinal ? ordinal_expect(s.thresholds, score) : score;
+}
 
 template <int VPL>
 __device__ __forceinline__ void predict_row(const DeviceState& s, const PredParams& pp, uint32_t u, uint32_t i,
@@ -75,7 +85,7 @@ __global__ void __launch_bounds__(kThreads) k_predict(DeviceState s, PredParams 
                 out[3 * r + 1] = sub[1];
                 out[3 * r + 2] = sub[2];
             } else {
-                float score = bp + dot + 0.0f;
+                const float score = finish_score(s, pp, bp, dot);
                 out[r] = offset ? score + offset[r] : score;
             }
         }
@@ -96,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) k_sse(DeviceState s, PredParams pp, 
         if (is_test && is_test[r] != 0) continue;
         float bp = 0.0f, dot = 0.0f;
         predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, nullptr);
-        const float e = (bp + dot + 0.0f) - target[r];
+        const float e = finish_score(s, pp, bp, dot) - target[r];
         const double ed = (double)e;
         sse += ed * ed;
         cnt += 1.0;
@@ -150,7 +160,7 @@ void predict_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, co
     tsvd_model* m = const_cast<tsvd_model*>(mc);
     if (n == 0) return;
     ProfScope ps(m, subscores ? "predict_subscores" : "predict");
-    PredParams pp{m->cfg.beta, m->cfg.low_memory};
+    PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
     const int vpl = (int)(m->d.Fs / 32);
     unsigned grid = (unsigned)std::min<uint64_t>((n + kWarps - 1) / kWarps, 148ull * 16);
     TSVD_DISPATCH(vpl, (k_predict<V><<<grid, kThreads, 0, m->stream>>>(m->d, pp, u, i, day, offset, n, out, subscores)));
@@ -162,7 +172,7 @@ void sse_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, const 
                 const int8_t* is_test, uint64_t n, double* out_sse, double* out_cnt) {
     tsvd_model* m = const_cast<tsvd_model*>(mc);
     ProfScope ps(m, "sse");
-    PredParams pp{m->cfg.beta, m->cfg.low_memory};
+    PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
     const int vpl = (int)(m->d.Fs / 32);
     DevMem part;
     part.alloc((2 * kSseBlocks + 2) * sizeof(double));

@@ -141,7 +141,19 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     if (tr.n_ratings >= (1ull << 32) || pr.n_ratings >= (1ull << 32))
         throw Error(TSVD_ERR_UNSUPPORTED, "at most 2^32-1 ratings per set");
     if (!c.low_memory) throw Error(TSVD_ERR_UNSUPPORTED, "low_memory = false (per-day NSVD1 terms) is not built yet");
-    if (c.has_ordinal_head) throw Error(TSVD_ERR_UNSUPPORTED, "the ordinal head is not built yet");
+    if (c.has_ordinal_head) {
+        // The reference moves the 4 shared thresholds after every rating
+        // (src/tx.rs:965-969), a serial chain over the whole epoch; every
+        // tsvdx4 job sets lr_t = 0, which is what is built.
+        if (c.ordinal_head.lr_t != 0.0f)
+            throw Error(TSVD_ERR_UNSUPPORTED, "ordinal head with lr_t != 0 (thresholds trained per rating)");
+        if (m->opts.schedule != TSVD_SCHED_HOGWILD)
+            throw Error(TSVD_ERR_UNSUPPORTED, "the ordinal head runs with the Hogwild schedule (tsvdx4p has none)");
+        if (!tr.raw_ratings) throw Error(TSVD_ERR_INVALID, "the ordinal head needs the training raw_ratings");
+        for (uint64_t t = 0; t < tr.n_ratings; ++t)
+            if (tr.raw_ratings[t] < 1 || tr.raw_ratings[t] > 5)
+                throw Error(TSVD_ERR_INVALID, "ordinal head: training rating outside 1..5");
+    }
 
     const uint32_t U = (uint32_t)tr.n_users, I = (uint32_t)tr.n_items;
     const uint64_t R = tr.n_ratings, P = pr.n_ratings;
@@ -211,6 +223,11 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     upload(d_pd, pr.dates, P, st);
     upload(m->m_user_off, uoff.data(), U + 1, st);
     upload(m->m_tu_mean, tum.data(), U, st);
+    s.raw = nullptr;
+    if (c.has_ordinal_head) {
+        upload(m->m_raw, tr.raw_ratings, R, st);
+        s.raw = m->m_raw.as<int8_t>();
+    }
     upload(m->m_ucnt_tr, tr.user_cnts, U, st);
     upload(m->m_ucnt_pr, pr.user_cnts, U, st);
     s.user_off = m->m_user_off.as<uint64_t>();
@@ -340,16 +357,25 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         clo.push_back(R);
         upload(m->m_chunk_lo, clo.data(), clo.size(), st);
         upload(m->m_item_chunk0, c0.data(), c0.size(), st);
-        m->m_chunk_part.alloc((size_t)s.n_chunks * Fs * 4);
-        m->m_chunk_epart.alloc((size_t)s.n_chunks * 4);
         s.chunk_lo = m->m_chunk_lo.as<uint64_t>();
         s.item_chunk0 = m->m_item_chunk0.as<uint32_t>();
-        s.chunk_part = m->m_chunk_part.as<float>();
-        s.chunk_epart = m->m_chunk_epart.as<float>();
         TSVD_CUDA(cudaStreamSynchronize(st));
     }
+    setup_params(m);
+}
 
-    // ---- parameters (TxModel::new field order, src/tx.rs:600-648) -----------
+// Per-model parameter tables and scratch (TxModel::new field order,
+// src/tx.rs:600-648). The dataset part of m->d (sizes, records, indices) must
+// already be set; models of one group share it and differ only here.
+void setup_params(tsvd_model* m) {
+    const tsvd_config& c = m->cfg;
+    cudaStream_t st = m->stream;
+    DeviceState& s = m->d;
+    const uint32_t U = s.n_users, I = s.n_items, F = s.F, Fs = s.Fs;
+    m->m_chunk_part.alloc((size_t)s.n_chunks * Fs * 4);
+    m->m_chunk_epart.alloc((size_t)s.n_chunks * 4);
+    s.chunk_part = m->m_chunk_part.as<float>();
+    s.chunk_epart = m->m_chunk_epart.as<float>();
     {
         const size_t NF = c.n_freq_bins, T = c.n_time_bins;
         ChaCha12Stream g(c.seed);
@@ -385,6 +411,16 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         zeros(m->m_e_user, U * 4, st);
         zeros(m->m_counters, 64, st);
         m->m_perm.alloc(U * 4);
+        if (m->opts.precision >= TSVD_PREC_BF16_READ) {
+            m->m_bf_ifeat.alloc((size_t)I * Fs * 2);
+            m->m_bf_qf0.alloc((size_t)I * Fs * 2);
+            m->m_bf_yfeat.alloc((size_t)I * Fs * 2);
+        }
+        if (m->opts.precision >= TSVD_PREC_BF16_READ_ALL) {
+            m->m_bf_ufeat.alloc((size_t)U * Fs * 2);
+            m->m_bf_ufeat2.alloc((size_t)U * Fs * 2);
+            m->m_bf_ycache.alloc((size_t)U * Fs * 2);
+        }
         s.ubias = m->m_ubias.as<float>(); s.ibias = m->m_ibias.as<float>();
         s.ufeat = m->m_ufeat.as<float>(); s.ufeat2 = m->m_ufeat2.as<float>();
         s.ifeat = m->m_ifeat.as<float>(); s.yfeat = m->m_yfeat.as<float>();
@@ -398,7 +434,10 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         s.thresholds = m->m_thresholds.as<float>();
         s.g_user = m->m_g_user.as<float>(); s.e_user = m->m_e_user.as<float>();
         s.counters = m->m_counters.as<uint32_t>();
-        s.raw = nullptr;
+        if (c.has_ordinal_head) {
+            TSVD_CUDA(cudaMemcpyAsync(m->m_thresholds.p, c.ordinal_head.th_init, 16, cudaMemcpyHostToDevice, st));
+            std::memcpy(m->h_thresholds, c.ordinal_head.th_init, 16);
+        }
     }
     TSVD_CUDA(cudaStreamSynchronize(st));
     m->ycache_valid = false;  // ycache starts at zero, as in the reference

@@ -17,7 +17,7 @@ import os
 
 import numpy as np
 
-from .abi import SCHED_HOGWILD, SCHED_STRATIFIED, PREC_FP32, TsvdGpuOptions, ptr
+from .abi import SCHED_HOGWILD, SCHED_STRATIFIED, PREC_FP32, TsvdConfig, TsvdGpuOptions, ptr
 from .config import TxConfig
 from .data import Dataset, MaskedDataset
 from .native import TsvdError, load
@@ -58,7 +58,21 @@ class TxModel:
     def new(cls, tr: Dataset, pr, cfg: TxConfig, **kw) -> "TxModel":
         return cls(tr, pr, cfg, **kw)
 
+    @classmethod
+    def _borrowed(cls, handle, cfg: TxConfig, n_users: int, n_items: int, owner) -> "TxModel":
+        """A view of a model owned by a TxGroup (never destroyed here)."""
+        m = cls.__new__(cls)
+        m._L = load()
+        m.cfg = cfg
+        m.n_users, m.n_items = n_users, n_items
+        m.h = handle
+        m._owner = owner
+        return m
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self.h = None
+            return
         if getattr(self, "h", None):
             self._L.tsvd_destroy(self.h)
             self.h = None
@@ -191,3 +205,65 @@ class TxModel:
         n = C.c_uint64()
         self._check(self._L.tsvd_launch_count(self.h, C.byref(n)))
         return n.value
+
+
+class TxGroup:
+    """Several TxModel variants over one device copy of the data, trained
+    together: one persistent launch per epoch (a CUDA graph from the second
+    epoch on). `models[k]` is the Regressor view of variant k."""
+
+    def __init__(self, tr: Dataset, pr, cfgs, device: int = 0):
+        L = load()
+        self._L = L
+        self.cfgs = list(cfgs)
+        n = len(self.cfgs)
+        arr = (TsvdConfig * n)(*[c.to_c() for c in self.cfgs])
+        opts = TsvdGpuOptions()
+        opts.schedule = SCHED_HOGWILD
+        opts.nsvd_norm_exp = 1.0
+        opts.device = device
+        tv = tr.view()
+        pv = pr.view() if isinstance(pr, MaskedDataset) else pr.view(masked=True)
+        h = C.c_void_p()
+        rc = L.tsvd_group_create(arr, n, C.byref(opts), C.byref(tv), C.byref(pv), C.byref(h))
+        if rc != 0:
+            raise TsvdError(rc, L.tsvd_group_last_error(None).decode())
+        self.h = h
+        self.models = []
+        for k in range(n):
+            mh = C.c_void_p()
+            self._check(L.tsvd_group_model(self.h, k, C.byref(mh)))
+            self.models.append(TxModel._borrowed(mh, self.cfgs[k], tr.n_users, tr.n_items, self))
+
+    def _check(self, rc):
+        if rc != 0:
+            raise TsvdError(rc, self._L.tsvd_group_last_error(self.h).decode())
+
+    def fit_epoch(self, epoch: int):
+        self._check(self._L.tsvd_group_fit_epoch(self.h, int(epoch)))
+
+    def set_graphs(self, on: bool):
+        self._check(self._L.tsvd_group_set_graphs(self.h, int(on)))
+
+    def last_epoch_ms(self) -> float:
+        out = C.c_double()
+        self._check(self._L.tsvd_group_last_epoch_ms(self.h, C.byref(out)))
+        return out.value
+
+    def autotune(self, sample_users: int = 2000):
+        out = np.zeros(len(self.cfgs), np.int32)
+        self._check(self._L.tsvd_group_autotune(self.h, sample_users, _p(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.models:
+                m.h = None
+            self._L.tsvd_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -21,6 +21,11 @@ EXPORTED = [
     "tsvd_rebuild_ycache", "tsvd_set_user_order", "tsvd_get_user_order", "tsvd_set_stream", "tsvd_synchronize",
     "tsvd_set_profiling", "tsvd_kernel_stats", "tsvd_reset_kernel_stats", "tsvd_launch_count", "tsvd_last_error",
     "tsvd_last_global_error", "tsvd_abi_version", "tsvd_user_order_for_seed", "tsvd_normal_stream",
+    "tsvd_group_create", "tsvd_group_destroy", "tsvd_group_size", "tsvd_group_model", "tsvd_group_fit_epoch",
+    "tsvd_group_set_graphs", "tsvd_group_last_epoch_ms", "tsvd_group_autotune", "tsvd_group_last_error",
+    "tsvd_encoder_create", "tsvd_encoder_destroy", "tsvd_encoder_train_epoch", "tsvd_encoder_loss_grad",
+    "tsvd_encoder_forward", "tsvd_encoder_apply", "tsvd_encoder_get", "tsvd_encoder_set",
+    "tsvd_encoder_target_stats", "tsvd_encoder_last_error", "tsvd_foldin", "tsvd_reset_users",
 ]
 
 _lib = None
@@ -73,6 +78,18 @@ def load():
     L.tsvd_abi_version.argtypes = []
     L.tsvd_user_order_for_seed.argtypes = [C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, P]
     L.tsvd_normal_stream.argtypes = [C.c_uint64, C.c_float, C.c_uint64, P]
+    L.tsvd_group_create.argtypes = [P, C.c_uint32, C.POINTER(TsvdGpuOptions), C.POINTER(TsvdDatasetView),
+                                    C.POINTER(TsvdDatasetView), C.POINTER(P)]
+    L.tsvd_group_destroy.argtypes = [P]
+    L.tsvd_group_destroy.restype = None
+    L.tsvd_group_size.argtypes = [P, C.POINTER(C.c_uint32)]
+    L.tsvd_group_model.argtypes = [P, C.c_uint32, C.POINTER(P)]
+    L.tsvd_group_fit_epoch.argtypes = [P, C.c_uint64]
+    L.tsvd_group_set_graphs.argtypes = [P, C.c_int32]
+    L.tsvd_group_last_epoch_ms.argtypes = [P, C.POINTER(C.c_double)]
+    L.tsvd_group_autotune.argtypes = [P, C.c_uint32, P]
+    L.tsvd_group_last_error.argtypes = [P]
+    L.tsvd_group_last_error.restype = C.c_char_p
     _lib = L
     return L
 

@@ -85,13 +85,14 @@ def _exact_total(rng, w: np.ndarray, total: int, lo: np.ndarray, hi: np.ndarray)
 
 def _argsort(key: np.ndarray) -> np.ndarray:
     """Stable argsort (identical result on every backend)."""
-    try:
-        import torch
-        if torch.cuda.is_available() and len(key) > (1 << 22):
-            t = torch.from_numpy(np.ascontiguousarray(key)).cuda()
-            return torch.sort(t, stable=True).indices.cpu().numpy()
-    except ImportError:
-        pass
+    if len(key) > (1 << 22):
+        try:
+            import torch
+            if torch.cuda.is_available():
+                t = torch.from_numpy(np.ascontiguousarray(key)).cuda()
+                return torch.sort(t, stable=True).indices.cpu().numpy()
+        except ImportError:
+            pass
     return np.argsort(key, kind="stable")
 
 

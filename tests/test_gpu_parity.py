@@ -125,6 +125,109 @@ def test_stratified_epoch_matches_oracle_tsvdx4p(small, f):
     assert abs(g.calc_rmse(pr) - o.calc_rmse(pr)) < 1e-5
 
 
+def disjoint_sets(n_users=64, per_user=70, seed=5):
+    """Users rate disjoint item blocks, so concurrent users never share an item
+    row: Hogwild is then race-free and must equal the sequential reference.
+    Several ratings per (user, day), in item order, exercise same-day updates
+    at varying distances."""
+    from netflix_prize_b200.data import Dataset
+    rng = np.random.default_rng(seed)
+    n_items = n_users * (per_user + 10)
+    tu, ti, tr_, td, pu, pi, pd_ = [], [], [], [], [], [], []
+    for u in range(n_users):
+        items = u * (per_user + 10) + np.arange(per_user + 10)
+        n_tr = int(rng.integers(per_user // 3, per_user))
+        days = np.sort(rng.choice(np.arange(100, 2000), size=max(2, n_tr // 5), replace=False))
+        d = rng.choice(days, size=n_tr)
+        tu += [u] * n_tr
+        ti += list(items[:n_tr])
+        tr_ += list(rng.integers(1, 6, n_tr))
+        td += list(d)
+        k = int(rng.integers(1, 8))
+        pu += [u] * k
+        pi += list(items[per_user:per_user + k])
+        pd_ += list(rng.choice(days, size=k))
+    tr = Dataset.from_ratings(tu, ti, tr_, td, n_users, n_items, "disjoint_tr")
+    o = np.lexsort((np.array(pu), np.array(pi)))
+    pr = Dataset.from_ratings(np.array(pu)[o], np.array(pi)[o], rng.integers(1, 6, len(pu)), np.array(pd_)[o],
+                              n_users, n_items, "disjoint_pr")
+    return tr, pr
+
+
+@pytest.mark.parametrize("f", [8, 64, 256])
+def test_hogwild_equals_sequential_reference_without_races(f):
+    tr, pr = disjoint_sets()
+    cfg = lm_cfg(f=f, epochs=2)
+    o = po.OracleModel(tr, MaskedDataset(pr), cfg)
+    g = TxModel(tr, MaskedDataset(pr), cfg, schedule=SCHED_HOGWILD)
+    for e in (1, 2):
+        o.fit_epoch(e, po.SCHED_SEQ)
+        g.fit_epoch(tr, pr, e)
+    for n in PARAMS + ["ycache", "ycache_bias"]:
+        a = np.asarray(g.get_param(n), np.float64).ravel()
+        b = np.asarray(o.get_param(n), np.float64).ravel()
+        assert np.max(np.abs(a - b)) < 2e-5, n
+    assert abs(g.calc_rmse(pr) - o.calc_rmse(pr)) < 1e-5
+
+
+def test_hogwild_ordinal_head_equals_sequential_without_races():
+    """The ordinal head (src/lib.rs:500-609) as the tsvdx4 `o` jobs use it:
+    lr_t = 0, thresholds sorted with a gap at each epoch end.  The initial
+    thresholds are sorted but 2.5 -> 2.6 is closer than the 0.25 gap, so the
+    epoch-end gap rule moves the third one.  (Unsorted thresholds make some
+    P(Y=y) negative; the 1e-6 clamp then scales that rating's gradient by 1e6
+    and the run measures exp() rounding rather than the schedule.)"""
+    from netflix_prize_b200.config import OrdinalHeadConfig
+    tr, pr = disjoint_sets(seed=9)
+    cfg = lm_cfg(f=32, epochs=2, ordinal_head=OrdinalHeadConfig((1.5, 2.5, 2.6, 4.5), 0.25, 0.0, 0.0))
+    o = po.OracleModel(tr, MaskedDataset(pr), cfg)
+    g = TxModel(tr, MaskedDataset(pr), cfg, schedule=SCHED_HOGWILD)
+    for e in (1, 2):
+        o.fit_epoch(e, po.SCHED_SEQ)
+        g.fit_epoch(tr, pr, e)
+    for n in PARAMS:
+        a = np.asarray(g.get_param(n), np.float64).ravel()
+        b = np.asarray(o.get_param(n), np.float64).ravel()
+        assert np.max(np.abs(a - b) - 1e-6 * np.abs(b)) < 2e-5, n
+    assert np.allclose(g.get_param("thresholds"), [1.5, 2.5, 2.75, 4.5], atol=1e-6, rtol=0)
+    assert np.allclose(g.get_param("thresholds"), o.get_param("thresholds"), atol=0, rtol=0)
+    want = o.predict_batch(pr.user_idxs, pr.item_idxs, pr.dates)
+    got = g.predict_batch(pr.user_idxs, pr.item_idxs, pr.dates)
+    assert np.max(np.abs(got - want)) < 1e-5
+    assert abs(g.calc_rmse(pr) - o.calc_rmse(pr)) < 1e-5
+
+
+@pytest.mark.parametrize("prec,rmse_tol,pred_tol", [(0, 2e-5, 2e-4), (1, 1e-3, 2e-2), (2, 1e-3, 2e-2)])
+def test_precision_forms_against_fp64_oracle(prec, rmse_tol, pred_tol):
+    """FP32 masters with FP32, BF16-item-table and BF16-everything read copies,
+    each stated against the FP64 oracle running the same stratified schedule."""
+    from netflix_prize_b200.abi import PREC_FP32
+    from tests.conftest import small_sets
+    tr, pr = small_sets(n_users=4000, n_items=1000, n_train=400000, seed=3)
+    cfg = run_lm(64, 6, n_time_bins=30)
+    o64 = po.OracleModel(tr, MaskedDataset(pr), cfg, fp64=True)
+    g = TxModel(tr, MaskedDataset(pr), cfg, schedule=SCHED_STRATIFIED, precision=prec)
+    for e in range(1, cfg.n_epochs + 1):
+        o64.fit_epoch(e, po.SCHED_P, nsvd_norm_exp=1.0, n_threads=1)
+        g.fit_epoch(tr, pr, e)
+    want = o64.predict_batch(pr.user_idxs, pr.item_idxs, pr.dates)
+    got = g.predict_batch(pr.user_idxs, pr.item_idxs, pr.dates).astype(np.float64)
+    err = np.abs(got - want)
+    r64, rg = o64.calc_rmse(pr), g.calc_rmse(pr)
+    print(f"precision {prec}: max|pred - fp64| {err.max():.3e} mean {err.mean():.3e}; "
+          f"rmse {rg:.6f} vs fp64 {r64:.6f} (diff {rg - r64:+.2e})")
+    assert abs(rg - r64) < rmse_tol
+    assert err.max() < pred_tol
+
+
+def test_bf16_copies_need_stratified(small):
+    from netflix_prize_b200.abi import PREC_BF16_READ
+    from netflix_prize_b200.native import TsvdError
+    tr, pr = small
+    with pytest.raises(TsvdError, match="stratified"):
+        TxModel(tr, MaskedDataset(pr), lm_cfg(), schedule=SCHED_HOGWILD, precision=PREC_BF16_READ)
+
+
 def test_stratified_is_bitwise_reproducible(small):
     tr, pr = small
     cfg = lm_cfg(f=32, epochs=2)

@@ -188,6 +188,27 @@ int tsvd_gen_preds(const tsvd_model* m, const tsvd_dataset_view* ds, float* out)
  * is_test == 0 rows of a full view. */
 int tsvd_calc_rmse(const tsvd_model* m, const tsvd_dataset_view* ds, double* out);
 
+/* Allocation-free RMSE over device-resident rows. No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they evaluate (memory reserved up front by the process owner, a caching
+ * allocator that must not be bypassed, or a latency-sensitive loop that may
+ * not call cudaMalloc/cudaFree, which can synchronise the device).
+ * Inputs d_u, d_i, d_day, d_target (and d_is_test, which may be NULL) are
+ * device arrays of n rows; d_out is a device array of 3 doubles that receives
+ * {rmse, sum of squared errors, rows counted} over the is_test == 0 rows.
+ * The result equals tsvd_calc_rmse's up to FP64 summation order.
+ * It calls no allocator: its scratch is a fixed 512 KiB device array inside
+ * the library (held by every GPU that loads it until exit), which limits n to
+ * 134,217,728 rows; larger n returns TSVD_ERR_INVALID. The scratch's device
+ * address is looked up on the first call on each device, so make that first
+ * call before any stream capture. Work is enqueued on the model's stream and
+ * not waited for. All calls share the scratch: calls that overlap on the GPU
+ * (different streams, no ordering between them) race and give wrong results. */
+int tsvd_calc_rmse_device_noalloc(const tsvd_model* m, const int32_t* d_u,
+                                  const int32_t* d_i, const int16_t* d_day,
+                                  const float* d_target, const int8_t* d_is_test,
+                                  uint64_t n, double* d_out);
+
 /* ---- parameters ------------------------------------------------------- */
 
 /* Names: gbias, ubias, ibias, ufeat, ufeat2, ifeat, yfeat, ycache, yfeat_day,

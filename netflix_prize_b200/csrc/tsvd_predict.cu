@@ -192,3 +192,141 @@ void sse_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, const 
 }
 
 }  // namespace tsvd
+
+// ===========================================================================
+// Allocation-free RMSE over device-resident rows.
+//
+// Some callers cannot allocate device memory at the time they need an
+// evaluation: a serving process whose memory is reserved up front by its
+// owner, code that runs under a caching allocator it must not bypass, or a
+// caller that sets all memory aside before a long job and forbids
+// cudaMalloc/cudaFree afterwards (both can also synchronise the device, which
+// a latency-sensitive caller avoids). tsvd_calc_rmse_device_noalloc serves
+// them: the caller passes device inputs and a device output, and the
+// reduction's scratch (per-tile partial sums) lives in the file-scope array
+// below, which every GPU that loads this library holds until the process
+// exits (kNoAllocScratchBytes = 512 KiB).
+// ===========================================================================
+namespace tsvd {
+namespace {
+
+constexpr uint32_t kNoAllocTileRows = 4096;   // rows per fixed tile (one block)
+constexpr uint32_t kNoAllocMaxTiles = 32768;  // => at most 134,217,728 rows per call
+constexpr uint64_t kNoAllocMaxRows = (uint64_t)kNoAllocTileRows * kNoAllocMaxTiles;
+
+}  // namespace
+}  // namespace tsvd
+
+// [2 * tile] = sum of squared errors of tile, [2 * tile + 1] = its row count.
+static __device__ __align__(256) double g_noalloc_scratch[2 * tsvd::kNoAllocMaxTiles];
+
+namespace tsvd {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = sizeof(double) * 2 * kNoAllocMaxTiles;
+static_assert(kNoAllocScratchBytes == 512 * 1024, "documented scratch size");
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[256] = {};  // device address of the scratch, per device ordinal
+
+// The scratch's device address on the current device. The array's name in host
+// code is only a host-side stand-in, so the address is looked up once per
+// device, with that device current, and cached.
+double* noalloc_scratch(int dev) {
+    if (dev < 0 || dev >= 256) throw Error(TSVD_ERR_INVALID, "device ordinal out of range for the no-alloc scratch");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            throw Error(TSVD_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    return g_noalloc_ptr[dev];
+}
+
+// One block per fixed tile of kNoAllocTileRows rows; warps take rows
+// w, w + 8, ...; the block's sums are combined in warp order. Every tile writes
+// both of its slots, so no slot needs clearing between calls.
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_sse_tiles(DeviceState s, PredParams pp, const int32_t* __restrict__ u,
+                                                        const int32_t* __restrict__ it, const int16_t* __restrict__ d,
+                                                        const float* __restrict__ target,
+                                                        const int8_t* __restrict__ is_test, uint64_t n,
+                                                        double* __restrict__ part) {
+    __shared__ double ssh[kWarps], csh[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t lo = (uint64_t)blockIdx.x * kNoAllocTileRows;
+    const uint64_t hi = lo + kNoAllocTileRows < n ? lo + kNoAllocTileRows : n;
+    double sse = 0.0, cnt = 0.0;
+    for (uint64_t r = lo + warp; r < hi; r += kWarps) {
+        if (is_test && is_test[r] != 0) continue;
+        float bp = 0.0f, dot = 0.0f;
+        predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, nullptr);
+        const double ed = (double)(finish_score(s, pp, bp, dot) - target[r]);
+        sse += ed * ed;
+        cnt += 1.0;
+    }
+    if (lane == 0) {
+        ssh[warp] = sse;
+        csh[warp] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            a += ssh[w];
+            c += csh[w];
+        }
+        part[2 * blockIdx.x] = a;
+        part[2 * blockIdx.x + 1] = c;
+    }
+}
+
+// Sums the tiles in order; out = {rmse, sse, count}.
+__global__ void k_sse_tiles_final(const double* __restrict__ part, uint32_t tiles, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (uint32_t t = 0; t < tiles; ++t) {
+            a += part[2 * t];
+            c += part[2 * t + 1];
+        }
+        out[0] = sqrt(a / c);
+        out[1] = a;
+        out[2] = c;
+    }
+}
+
+}  // namespace
+}  // namespace tsvd
+
+extern "C" int tsvd_calc_rmse_device_noalloc(const tsvd_model* m, const int32_t* d_u, const int32_t* d_i,
+                                             const int16_t* d_day, const float* d_target, const int8_t* d_is_test,
+                                             uint64_t n, double* d_out) {
+    using namespace tsvd;
+    if (!m) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(m->mu);
+    try {
+        if (!d_u || !d_i || !d_day || !d_target || !d_out) throw Error(TSVD_ERR_INVALID, "null device pointer");
+        if (n == 0) throw Error(TSVD_ERR_INVALID, "no rows");
+        if (n > kNoAllocMaxRows)
+            throw Error(TSVD_ERR_INVALID, "tsvd_calc_rmse_device_noalloc: " + std::to_string(n) +
+                                              " rows exceed the maximum of " + std::to_string(kNoAllocMaxRows) +
+                                              " (its fixed scratch holds " + std::to_string(kNoAllocMaxTiles) +
+                                              " tiles of " + std::to_string(kNoAllocTileRows) + " rows)");
+        TSVD_CUDA(cudaSetDevice(m->device));
+        double* part = noalloc_scratch(m->device);
+        const uint32_t tiles = (uint32_t)((n + kNoAllocTileRows - 1) / kNoAllocTileRows);
+        PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
+        const int vpl = (int)(m->d.Fs / 32);
+        TSVD_DISPATCH(vpl, (k_sse_tiles<V><<<tiles, kThreads, 0, m->stream>>>(m->d, pp, d_u, d_i, d_day, d_target,
+                                                                              d_is_test, n, part)));
+        k_sse_tiles_final<<<1, 32, 0, m->stream>>>(part, tiles, d_out);
+        TSVD_CUDA(cudaGetLastError());
+        const_cast<tsvd_model*>(m)->launches += 2;
+        return TSVD_OK;
+    } catch (const Error& e) {
+        m->err = e.what();
+        return e.status;
+    }
+}

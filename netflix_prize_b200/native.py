@@ -21,6 +21,7 @@ EXPORTED = [
     "tsvd_rebuild_ycache", "tsvd_set_user_order", "tsvd_get_user_order", "tsvd_set_stream", "tsvd_synchronize",
     "tsvd_set_profiling", "tsvd_kernel_stats", "tsvd_reset_kernel_stats", "tsvd_launch_count", "tsvd_last_error",
     "tsvd_last_global_error", "tsvd_abi_version", "tsvd_user_order_for_seed", "tsvd_normal_stream",
+    "tsvd_calc_rmse_device_noalloc",
     "tsvd_group_create", "tsvd_group_destroy", "tsvd_group_size", "tsvd_group_model", "tsvd_group_fit_epoch",
     "tsvd_group_set_graphs", "tsvd_group_last_epoch_ms", "tsvd_group_autotune", "tsvd_group_last_error",
     "tsvd_encoder_create", "tsvd_encoder_destroy", "tsvd_encoder_train_epoch", "tsvd_encoder_loss_grad",
@@ -78,6 +79,7 @@ def load():
     L.tsvd_abi_version.argtypes = []
     L.tsvd_user_order_for_seed.argtypes = [C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, P]
     L.tsvd_normal_stream.argtypes = [C.c_uint64, C.c_float, C.c_uint64, P]
+    L.tsvd_calc_rmse_device_noalloc.argtypes = [P, P, P, P, P, P, C.c_uint64, P]
     L.tsvd_group_create.argtypes = [P, C.c_uint32, C.POINTER(TsvdGpuOptions), C.POINTER(TsvdDatasetView),
                                     C.POINTER(TsvdDatasetView), C.POINTER(P)]
     L.tsvd_group_destroy.argtypes = [P]

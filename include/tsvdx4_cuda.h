@@ -112,7 +112,12 @@ enum tsvd_schedule {
      * item tables frozen, NSVD1 deltas reduced in a fixed order), then an
      * item stratum (items in parallel, user tables frozen). Bitwise
      * reproducible for a given seed. */
-    TSVD_SCHED_STRATIFIED = 1
+    TSVD_SCHED_STRATIFIED = 1,
+    /* The reference's sequential pass exactly (src/tx.rs:756-1106): one warp
+     * takes the users one after another in get_users order, so every rating
+     * sees every earlier update. Slow (one warp on the GPU); for parity runs
+     * and small data. */
+    TSVD_SCHED_SEQUENTIAL = 2
 };
 
 /* Precision forms (stratified schedule only: its strata read frozen tables).

@@ -18,6 +18,7 @@ TSVD_ERR_TIMEOUT = 6
 
 SCHED_HOGWILD = 0
 SCHED_STRATIFIED = 1
+SCHED_SEQUENTIAL = 2
 PREC_FP32 = 0
 PREC_BF16_READ = 1
 PREC_BF16_READ_ALL = 2

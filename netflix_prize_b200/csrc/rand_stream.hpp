@@ -49,6 +49,9 @@ class ChaCha12Stream {
         uint64_t lo = u32();
         return lo | ((uint64_t)u32() << 32);
     }
+    // The 256-bit ChaCha key the seed expands to (for device-side generation
+    // of the same keystream).
+    const uint32_t* key() const { return key_; }
 
   private:
     static constexpr int kBlocks = 4, kWords = 16 * kBlocks;

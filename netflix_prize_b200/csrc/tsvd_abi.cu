@@ -56,6 +56,9 @@ bool find_param(const tsvd_model* m, const std::string& n, ParamRef& r) {
     if (n == "ybias") return set(s.ybias, 1, I, I);
     if (n == "ycache_bias") return set(s.ycache_bias, 1, U, U);
     if (n == "ubias_day") return set(s.ubias_day, 1, UD, UD);
+    if (n == "yfeat_day" && s.yfeat_day) return set(s.yfeat_day, I, F, Fs);
+    if (n == "ufeat_day" && s.ufeat_day) return set(s.ufeat_day, UD, F, Fs);
+    if (n == "ycache_day" && s.ycache_day) return set(s.ycache_day, UD, F, Fs);
     if (n == "ibias_freq") return set(s.ibias_freq, I, NF, NF);
     if (n == "ifeat_freq") return set(s.ifeat_freq, I * NF, F, Fs);
     if (n == "cu") return set(s.cu, 1, U, U);
@@ -131,7 +134,8 @@ int tsvd_create(const tsvd_config* cfg, const tsvd_gpu_options* opts, const tsvd
             std::memset(&m->opts, 0, sizeof(m->opts));
             m->opts.nsvd_norm_exp = 1.0f;
         }
-        if (m->opts.schedule != TSVD_SCHED_HOGWILD && m->opts.schedule != TSVD_SCHED_STRATIFIED)
+        if (m->opts.schedule != TSVD_SCHED_HOGWILD && m->opts.schedule != TSVD_SCHED_STRATIFIED &&
+            m->opts.schedule != TSVD_SCHED_SEQUENTIAL)
             throw Error(TSVD_ERR_INVALID, "unknown schedule");
         if (m->opts.precision < TSVD_PREC_FP32 || m->opts.precision > TSVD_PREC_BF16_READ_ALL)
             throw Error(TSVD_ERR_INVALID, "unknown precision");
@@ -350,6 +354,7 @@ int tsvd_rebuild_ycache(tsvd_model* m) {
     return guarded(m, [&] {
         use_device(m);
         tsvd::rebuild_ycache(m);
+        tsvd::rebuild_ycache_day(m);
         TSVD_CUDA(cudaStreamSynchronize(m->stream));
     });
 }

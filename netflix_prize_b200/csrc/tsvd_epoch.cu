@@ -29,6 +29,10 @@ EpochParams make_params(const tsvd_model* m) {
     p.lr_ta = c.lr_ta; p.lr_ibf = c.lr_ibf; p.lr_iqf = c.lr_iqf; p.lr_cu = c.lr_cu;
     p.reg_iqf = c.reg_iqf; p.reg_cu = c.reg_cu; p.reg_u = c.reg_u; p.reg_u2 = c.reg_u2; p.reg_i = c.reg_i;
     p.reg_y = c.reg_y;
+    p.lr_ud = c.lr_ud; p.reg_ud = c.reg_ud; p.lr_yd = c.lr_yd; p.reg_yd = c.reg_yd;
+    p.lr_t = c.has_ordinal_head ? c.ordinal_head.lr_t : 0.0f;
+    p.reg_t = c.has_ordinal_head ? c.ordinal_head.reg_t : 0.0f;
+    p.has_ud = (!c.low_memory && c.lr_ud != 0.0f) ? 1 : 0;
     p.w_bias = c.w_bias; p.w_factor = c.w_factor;
     p.nsvd_norm_exp = m->opts.nsvd_norm_exp;
     p.sum_err_bug = c.sum_err_bug;
@@ -54,34 +58,6 @@ namespace {
 //  - the su gather and the end-of-user y update keep 8 rows in flight.
 // ---------------------------------------------------------------------------
 constexpr int kStages = 4;  // default ring depth (the batched form tunes it per width)
-constexpr int kBatch = 8;
-
-// su += y_j for the items given by item_of(0..n-1), in order, 8 rows in flight.
-template <int VPL, class ItemOf>
-__device__ __forceinline__ void gather_y8(const DeviceState& s, uint64_t n, ItemOf item_of, int lane,
-                                          float (&su)[VPL], float& sub) {
-    for (uint64_t base = 0; base < n; base += 32) {
-        const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
-        const uint32_t mine = lane < (int)cnt ? item_of(base + lane) : 0u;
-        for (uint32_t j = 0; j < cnt; j += kBatch) {
-            float y[kBatch][VPL], yb[kBatch];
-#pragma unroll
-            for (int q = 0; q < kBatch; ++q) {
-                const uint32_t it = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
-                Row<VPL>::load_cg(s.yfeat + (size_t)it * s.Fs, lane, y[q]);
-                yb[q] = __ldcg(s.ybias + it);
-            }
-#pragma unroll
-            for (int q = 0; q < kBatch; ++q) {
-                if (j + q < cnt) {
-#pragma unroll
-                    for (int v = 0; v < VPL; ++v) su[v] += y[q][v];
-                    sub += yb[q];
-                }
-            }
-        }
-    }
-}
 
 // One user of a Hogwild epoch, by one warp; `ring` is the warp's
 // ST * (2 Fs + 8)-float shared-memory slice; ratings are staged ST - 1 ahead.
@@ -542,7 +518,7 @@ void run_epoch(tsvd_model* m, uint64_t epoch) {
         TSVD_CUDA(cudaMemsetAsync(m->d.ufeat2, 0, m->m_ufeat2.bytes, m->stream));
     }
     reset_counters(m);
-    if (m->opts.schedule == TSVD_SCHED_HOGWILD) {
+    if (m->opts.schedule == TSVD_SCHED_HOGWILD || m->opts.schedule == TSVD_SCHED_SEQUENTIAL) {
         // per-epoch user order: injected, or get_users (src/lib.rs:486-494)
         std::vector<uint32_t> order;
         auto it = m->injected_order.find(epoch);
@@ -550,11 +526,19 @@ void run_epoch(tsvd_model* m, uint64_t epoch) {
         else order = user_order(m->d.n_users, c.shuffle_users != 0, c.seed, epoch);
         TSVD_CUDA(cudaMemcpyAsync(m->m_perm.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, m->stream));
         TSVD_CUDA(cudaStreamSynchronize(m->stream));  // `order` leaves scope
-        {
+        if (m->opts.schedule == TSVD_SCHED_SEQUENTIAL || !c.low_memory) {
+            day_epoch_pass(m, m->m_perm.as<uint32_t>(), m->opts.schedule == TSVD_SCHED_SEQUENTIAL);
+        } else {
             ProfScope ps(m, "user_pass_hogwild");
             TSVD_DISPATCH(vpl, launch_hog_pass<V>(m, p, m->m_perm.as<uint32_t>()));
         }
         rebuild_ycache(m);
+        rebuild_ycache_day(m);
+        if (c.has_ordinal_head && c.ordinal_head.lr_t != 0.0f) {
+            // thresholds moved on the device during the pass
+            TSVD_CUDA(cudaMemcpyAsync(m->h_thresholds, m->d.thresholds, 16, cudaMemcpyDeviceToHost, m->stream));
+            TSVD_CUDA(cudaStreamSynchronize(m->stream));
+        }
     } else {
         p.use_ycache = (c.full_su && m->ycache_valid) ? 1 : 0;
         stratified_epoch(m, p);

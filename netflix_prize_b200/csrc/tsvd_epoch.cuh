@@ -16,6 +16,9 @@ constexpr uint32_t kSlotScalars = 12;
 struct EpochParams {
     float lr_u, lr_u2, lr_ub, lr_ubd, lr_i, lr_ib, lr_y, lr_yb, lr_tu, lr_ti, lr_ta, lr_ibf, lr_iqf, lr_cu;
     float reg_iqf, reg_cu, reg_u, reg_u2, reg_i, reg_y;
+    float lr_ud, reg_ud, lr_yd, reg_yd;  // per-day terms (low_memory = false)
+    float lr_t, reg_t;                   // ordinal-head thresholds (sequential schedule)
+    int32_t has_ud;                      // ufeat_day trained: !low_memory && lr_ud != 0
     float w_bias, w_factor;
     float nsvd_norm_exp;
     int32_t sum_err_bug;
@@ -31,6 +34,43 @@ void launch_hog_batched(cudaStream_t st, const DeviceState* d_states, const Epoc
 void launch_rebuild_batched(cudaStream_t st, const DeviceState* d_states, uint32_t n_models, uint32_t n_users);
 
 EpochParams make_params(const tsvd_model* m);
+
+constexpr int kBatch = 8;  // feature rows in flight in the y gathers and updates
+
+// su += y_j (and sub += b_j when yb is given) for the items item_of(0..n-1)
+// of table y, added in order, kBatch rows in flight.
+template <int VPL, class ItemOf>
+__device__ __forceinline__ void gather_rows8(const float* y_tab, const float* yb_tab, uint32_t Fs, uint64_t n,
+                                             ItemOf item_of, int lane, float (&su)[VPL], float& sub) {
+    for (uint64_t base = 0; base < n; base += 32) {
+        const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
+        const uint32_t mine = lane < (int)cnt ? item_of(base + lane) : 0u;
+        for (uint32_t j = 0; j < cnt; j += kBatch) {
+            float y[kBatch][VPL], yb[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const uint32_t it = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
+                Row<VPL>::load_cg(y_tab + (size_t)it * Fs, lane, y[q]);
+                yb[q] = yb_tab ? __ldcg(yb_tab + it) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                if (j + q < cnt) {
+#pragma unroll
+                    for (int v = 0; v < VPL; ++v) su[v] += y[q][v];
+                    sub += yb[q];
+                }
+            }
+        }
+    }
+}
+
+// su += y_j, sub += b_j over the NSVD1 table y (yfeat, ybias).
+template <int VPL, class ItemOf>
+__device__ __forceinline__ void gather_y8(const DeviceState& s, uint64_t n, ItemOf item_of, int lane,
+                                          float (&su)[VPL], float& sub) {
+    gather_rows8<VPL>(s.yfeat, s.ybias, s.Fs, n, item_of, lane, su, sub);
+}
 
 // BF16 read copies of FP32 master rows (same padded layout, 2 bytes/element).
 struct Bf16Copies {

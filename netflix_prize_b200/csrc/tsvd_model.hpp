@@ -102,6 +102,11 @@ struct DeviceState {
     const int16_t* ud_date;    // [n_ud]
     const uint32_t* ud_cnt;    // [n_ud]
     const float* tu_mean;      // [U]
+    // (user, day) item lists, low_memory = false: per ud, its pr items in pr
+    // order, then its training items in training order
+    const uint64_t* ud_list_off;   // [n_ud + 1]
+    const uint32_t* ud_list_item;  // [n_train + n_pr]
+    const uint32_t* ud_pr_cnt;     // [n_ud] pr items at the front of each list
     // parameters (feature rows have stride Fs, zero padded)
     float *ubias, *ibias, *ufeat, *ufeat2, *ifeat, *yfeat, *ycache, *yfeat_day;
     float *alpha_u, *but_bin, *bit_bin, *ybias, *ycache_bias;
@@ -148,6 +153,7 @@ struct tsvd_model {
     // device allocations
     tsvd::DevMem m_rec, m_user_off, m_irec, m_item_off, m_pr_item, m_pr_off, m_ucnt_tr, m_ucnt_pr, m_raw;
     tsvd::DevMem m_ud_start, m_ud_date, m_ud_cnt, m_tu_mean;
+    tsvd::DevMem m_ud_list_off, m_ud_list_item, m_ud_pr_cnt;
     tsvd::DevMem m_ubias, m_ibias, m_ufeat, m_ufeat2, m_ifeat, m_yfeat, m_ycache, m_yfeat_day;
     tsvd::DevMem m_alpha_u, m_but_bin, m_bit_bin, m_ybias, m_ycache_bias;
     tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
@@ -173,6 +179,17 @@ namespace tsvd {
 // setup (tsvd_setup.cu)
 void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_view& pr);
 void setup_params(tsvd_model* m);
+// seeded normal init on the device (tsvd_init.cu)
+struct NormalTable {
+    float* dst;       // rows x stride floats; columns cols..stride-1 are zeroed
+    uint64_t rows;
+    uint32_t cols, stride;
+    float sigma;
+};
+void device_normal_tables(const NormalTable* tables, int n_tables, uint64_t seed, cudaStream_t st);
+// per-day terms, low_memory = false (tsvd_day.cu)
+void day_epoch_pass(tsvd_model* m, const uint32_t* order, bool sequential);
+void rebuild_ycache_day(tsvd_model* m);
 // epoch drivers (tsvd_epoch.cu)
 void run_epoch(tsvd_model* m, uint64_t epoch);
 void rebuild_ycache(tsvd_model* m);

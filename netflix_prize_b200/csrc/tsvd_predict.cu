@@ -47,13 +47,25 @@ __device__ __forceinline__ void predict_row(const DeviceState& s, const PredPara
     Row<VPL>::load_nc(s.ycache + (size_t)u * Fs, lane, su);
     Row<VPL>::load_nc(s.ifeat + (size_t)i * Fs, lane, q);
     Row<VPL>::load_nc(s.ifeat_freq + ((size_t)i * NF + f) * Fs, lane, qf);
+    // per-day terms, low_memory = false (src/tx.rs:329-334, :692-699)
+    const bool per_day = !pp.low_memory && has;
+    float pd[VPL], sd[VPL];
+    if (per_day) {
+        Row<VPL>::load_nc(s.ufeat_day + (size_t)idx * Fs, lane, pd);
+        Row<VPL>::load_nc(s.ycache_day + (size_t)idx * Fs, lane, sd);
+    }
     if (subs) {
         float mf = 0.0f, ns = 0.0f;
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
             const float qe = q[v] + qf[v];
-            mf += (pu[v] + dv * p2[v]) * qe;
-            ns += su[v] * qe;
+            float pe = pu[v] + dv * p2[v], se = su[v];
+            if (per_day) {
+                pe += pd[v];
+                se += sd[v];
+            }
+            mf += pe * qe;
+            ns += se * qe;
         }
         mf = warp_sum(mf);
         ns = warp_sum(ns);
@@ -63,7 +75,14 @@ __device__ __forceinline__ void predict_row(const DeviceState& s, const PredPara
     } else {
         float part = 0.0f;
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) part += ((pu[v] + su[v]) + dv * p2[v]) * (q[v] + qf[v]);
+        for (int v = 0; v < VPL; ++v) {
+            float pe = (pu[v] + su[v]) + dv * p2[v];
+            if (per_day) {
+                pe += pd[v];
+                pe += sd[v];
+            }
+            part += pe * (q[v] + qf[v]);
+        }
         dot = warp_sum(part);
         bias_part = s.gbias + bu_t + bi_t * cu_t;
     }

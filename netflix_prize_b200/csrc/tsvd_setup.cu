@@ -88,6 +88,40 @@ __global__ void k_fill(float* __restrict__ v, uint64_t n, float x) {
         v[k] = x;
 }
 
+// (user, day) keys of the per-ud item lists: pr rows first (pr order), then
+// training rows (training order); values are the items. Counts pr rows per ud.
+__global__ void k_ud_list_keys(DeviceState s, const int32_t* __restrict__ pu, const int32_t* __restrict__ pi,
+                               const int16_t* __restrict__ pd, uint64_t P, uint32_t* __restrict__ key,
+                               uint32_t* __restrict__ val, uint32_t* __restrict__ pr_cnt) {
+    const uint64_t n = P + s.n_train;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        if (k < P) {
+            const uint32_t ud = ud_index(s, (uint32_t)pu[k], pd[k]);  // present: SparseUD covers pr
+            key[k] = ud;
+            val[k] = (uint32_t)pi[k];
+            atomicAdd(pr_cnt + ud, 1u);
+        } else {
+            const Rec r = s.rec[k - P];
+            key[k] = r.ud;
+            val[k] = rec_id(r.key);
+        }
+    }
+}
+
+// off[d] = first k with keys[k] >= d, for d in [0, n_ud].
+__global__ void k_lower_bound_u32(const uint32_t* __restrict__ keys, uint64_t n, uint64_t n_ud,
+                                  uint64_t* __restrict__ off) {
+    for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d <= n_ud; d += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (keys[mid] < d) lo = mid + 1;
+            else hi = mid;
+        }
+        off[d] = lo;
+    }
+}
+
 constexpr unsigned kGrid = 148 * 8, kBlock = 256;
 
 template <class T>
@@ -140,15 +174,19 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     if (tr.n_ratings == 0) throw Error(TSVD_ERR_INVALID, "empty training set");
     if (tr.n_ratings >= (1ull << 32) || pr.n_ratings >= (1ull << 32))
         throw Error(TSVD_ERR_UNSUPPORTED, "at most 2^32-1 ratings per set");
-    if (!c.low_memory) throw Error(TSVD_ERR_UNSUPPORTED, "low_memory = false (per-day NSVD1 terms) is not built yet");
+    if (!c.low_memory && m->opts.schedule == TSVD_SCHED_STRATIFIED)
+        throw Error(TSVD_ERR_UNSUPPORTED,
+                    "low_memory = false (per-day NSVD1 terms) runs with the Hogwild or sequential schedule");
     if (c.has_ordinal_head) {
         // The reference moves the 4 shared thresholds after every rating
         // (src/tx.rs:965-969), a serial chain over the whole epoch; every
         // tsvdx4 job sets lr_t = 0, which is what is built.
-        if (c.ordinal_head.lr_t != 0.0f)
-            throw Error(TSVD_ERR_UNSUPPORTED, "ordinal head with lr_t != 0 (thresholds trained per rating)");
-        if (m->opts.schedule != TSVD_SCHED_HOGWILD)
-            throw Error(TSVD_ERR_UNSUPPORTED, "the ordinal head runs with the Hogwild schedule (tsvdx4p has none)");
+        if (m->opts.schedule == TSVD_SCHED_STRATIFIED)
+            throw Error(TSVD_ERR_UNSUPPORTED,
+                        "the ordinal head runs with the Hogwild or sequential schedule (tsvdx4p has none)");
+        if (c.ordinal_head.lr_t != 0.0f && m->opts.schedule != TSVD_SCHED_SEQUENTIAL)
+            throw Error(TSVD_ERR_UNSUPPORTED,
+                        "ordinal head with lr_t != 0 (thresholds trained per rating) needs the sequential schedule");
         if (!tr.raw_ratings) throw Error(TSVD_ERR_INVALID, "the ordinal head needs the training raw_ratings");
         for (uint64_t t = 0; t < tr.n_ratings; ++t)
             if (tr.raw_ratings[t] < 1 || tr.raw_ratings[t] > 5)
@@ -286,6 +324,35 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     TSVD_CUDA(cudaGetLastError());
     s.rec = m->m_rec.as<Rec>();
 
+    // ---- per-(user, day) item lists for the per-day terms (low_memory = false):
+    // probe_items_by_ud (src/tx.rs:587-598) and the rebuild_ycache_day order
+    // (src/tx.rs:420-454) in one sorted list per ud
+    s.ud_list_off = nullptr;
+    s.ud_list_item = nullptr;
+    s.ud_pr_cnt = nullptr;
+    if (!c.low_memory) {
+        const uint64_t N = R + P, n_ud = s.n_ud;
+        DevMem key, key_sorted, val;
+        key.alloc(N * 4);
+        key_sorted.alloc(N * 4);
+        val.alloc(N * 4);
+        m->m_ud_list_item.alloc(N * 4);
+        m->m_ud_list_off.alloc((n_ud + 1) * 8);
+        zeros(m->m_ud_pr_cnt, n_ud * 4, st);
+        k_ud_list_keys<<<kGrid, kBlock, 0, st>>>(s, d_pu.as<int32_t>(), d_pi.as<int32_t>(), d_pd.as<int16_t>(), P,
+                                                 key.as<uint32_t>(), val.as<uint32_t>(), m->m_ud_pr_cnt.as<uint32_t>());
+        TSVD_CUDA(cudaGetLastError());
+        sort_pairs(tmp, key.as<uint32_t>(), key_sorted.as<uint32_t>(), val.as<uint32_t>(),
+                   m->m_ud_list_item.as<uint32_t>(), N, bits_for(n_ud), st);
+        k_lower_bound_u32<<<ceil_div(n_ud + 1, kBlock), kBlock, 0, st>>>(key_sorted.as<uint32_t>(), N, n_ud,
+                                                                         m->m_ud_list_off.as<uint64_t>());
+        TSVD_CUDA(cudaGetLastError());
+        s.ud_list_off = m->m_ud_list_off.as<uint64_t>();
+        s.ud_list_item = m->m_ud_list_item.as<uint32_t>();
+        s.ud_pr_cnt = m->m_ud_pr_cnt.as<uint32_t>();
+        TSVD_CUDA(cudaStreamSynchronize(st));
+    }
+
     // ---- pr items grouped by user, pr order kept (probe_items_by_user) ------
     {
         DevMem idx, idx_sorted, ukey, ukey_sorted;
@@ -378,20 +445,26 @@ void setup_params(tsvd_model* m) {
     s.chunk_epart = m->m_chunk_epart.as<float>();
     {
         const size_t NF = c.n_freq_bins, T = c.n_time_bins;
-        ChaCha12Stream g(c.seed);
-        std::vector<float> h;
-        auto normal_table = [&](DevMem& dst, size_t rows, float sigma) {
-            h.assign(rows * Fs, 0.0f);
-            fill_normal_rows(g, sigma, rows, F, h.data(), Fs);
-            upload(dst, h.data(), h.size(), st);
-            TSVD_CUDA(cudaStreamSynchronize(st));  // h is reused
-        };
-        normal_table(m->m_ufeat, U, c.sigma_u);
+        // rand_array2 draws, in TxModel::new order, from one seeded stream:
+        // ufeat, ifeat, yfeat, yfeat_day (low_memory = false only), then
+        // (after the zero tables) ifeat_freq
+        m->m_ufeat.alloc((size_t)U * Fs * 4);
+        m->m_ifeat.alloc((size_t)I * Fs * 4);
+        m->m_yfeat.alloc((size_t)I * Fs * 4);
+        m->m_ifeat_freq.alloc((size_t)I * NF * Fs * 4);
+        std::vector<NormalTable> drawn = {{m->m_ufeat.as<float>(), U, F, Fs, c.sigma_u},
+                                          {m->m_ifeat.as<float>(), I, F, Fs, c.sigma_i},
+                                          {m->m_yfeat.as<float>(), I, F, Fs, c.sigma_y}};
+        if (!c.low_memory) {
+            m->m_yfeat_day.alloc((size_t)I * Fs * 4);
+            drawn.push_back({m->m_yfeat_day.as<float>(), I, F, Fs, c.sigma_yd});
+            zeros(m->m_ufeat_day, (size_t)s.n_ud * Fs * 4, st);
+            zeros(m->m_ycache_day, (size_t)s.n_ud * Fs * 4, st);
+        }
+        drawn.push_back({m->m_ifeat_freq.as<float>(), (uint64_t)I * NF, F, Fs, c.sigma_iqf});
+        device_normal_tables(drawn.data(), (int)drawn.size(), c.seed, st);
         zeros(m->m_ufeat2, (size_t)U * Fs * 4, st);
-        normal_table(m->m_ifeat, I, c.sigma_i);
-        normal_table(m->m_yfeat, I, c.sigma_y);
         zeros(m->m_ycache, (size_t)U * Fs * 4, st);
-        // yfeat_day would be drawn here when !low_memory
         zeros(m->m_alpha_u, U * 4, st);
         zeros(m->m_but_bin, (size_t)U * T * 4, st);
         zeros(m->m_bit_bin, (size_t)I * T * 4, st);
@@ -399,7 +472,6 @@ void setup_params(tsvd_model* m) {
         zeros(m->m_ycache_bias, U * 4, st);
         zeros(m->m_ubias_day, s.n_ud * 4, st);
         zeros(m->m_ibias_freq, (size_t)I * NF * 4, st);
-        normal_table(m->m_ifeat_freq, (size_t)I * NF, c.sigma_iqf);
         zeros(m->m_ubias, U * 4, st);
         zeros(m->m_ibias, I * 4, st);
         m->m_cu.alloc(U * 4);
@@ -424,11 +496,13 @@ void setup_params(tsvd_model* m) {
         s.ubias = m->m_ubias.as<float>(); s.ibias = m->m_ibias.as<float>();
         s.ufeat = m->m_ufeat.as<float>(); s.ufeat2 = m->m_ufeat2.as<float>();
         s.ifeat = m->m_ifeat.as<float>(); s.yfeat = m->m_yfeat.as<float>();
-        s.ycache = m->m_ycache.as<float>(); s.yfeat_day = nullptr;
+        s.ycache = m->m_ycache.as<float>();
+        s.yfeat_day = c.low_memory ? nullptr : m->m_yfeat_day.as<float>();
         s.alpha_u = m->m_alpha_u.as<float>(); s.but_bin = m->m_but_bin.as<float>();
         s.bit_bin = m->m_bit_bin.as<float>(); s.ybias = m->m_ybias.as<float>();
         s.ycache_bias = m->m_ycache_bias.as<float>(); s.ubias_day = m->m_ubias_day.as<float>();
-        s.ufeat_day = nullptr; s.ycache_day = nullptr;
+        s.ufeat_day = c.low_memory ? nullptr : m->m_ufeat_day.as<float>();
+        s.ycache_day = c.low_memory ? nullptr : m->m_ycache_day.as<float>();
         s.ibias_freq = m->m_ibias_freq.as<float>(); s.ifeat_freq = m->m_ifeat_freq.as<float>();
         s.cu = m->m_cu.as<float>(); s.cut = m->m_cut.as<float>();
         s.thresholds = m->m_thresholds.as<float>();

@@ -47,6 +47,21 @@ def test_initial_state_bitwise(small):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
 
 
+def test_initial_state_bitwise_12m_draws():
+    """The device-side init at f=256 over ~12M normal draws (about 150k
+    ziggurat wedge tests and a few thousand tail draws) equals the
+    sequential host stream bit for bit."""
+    from tests.conftest import small_sets
+    tr, pr = small_sets(n_users=40000, n_items=400, n_train=200000, seed=5)
+    cfg = lm_cfg(f=256, epochs=1)
+    g = TxModel(tr, MaskedDataset(pr), cfg)
+    o = po.OracleModel(tr, MaskedDataset(pr), cfg)
+    for n in ["ufeat", "ifeat", "yfeat", "ifeat_freq"]:
+        a = np.asarray(g.get_param(n), np.float32).ravel()
+        b = np.asarray(o.get_param(n), np.float32).ravel()
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
+
+
 def test_user_order_matches_reference_shuffle(small):
     tr, pr = small
     g = TxModel(tr, MaskedDataset(pr), lm_cfg())

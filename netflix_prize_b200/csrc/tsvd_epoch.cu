@@ -59,225 +59,227 @@ namespace {
 // ---------------------------------------------------------------------------
 constexpr int kStages = 4;  // default ring depth (the batched form tunes it per width)
 
-// One user of a Hogwild epoch, by one warp; `ring` is the warp's
-// ST * (2 Fs + 8)-float shared-memory slice; ratings are staged ST - 1 ahead.
+// One user of a Hogwild epoch, by one warp. `ring` is the warp's
+// hog_ring_floats(ST, Fs) floats of shared memory: ST staging slots (q row,
+// q^f row, four item-side scalars) followed by a window of kRecWindow of the
+// user's rating records. Ratings are staged ST - 1 ahead.
+//
+// The user-side updates use x - lr (g + reg x) = (1 - lr reg) x - lr g, with
+// the constant factor hoisted out of the rating loop; the item-side deltas
+// likewise. Same arithmetic as the reference up to FP32 rounding.
 template <int VPL, int ST = kStages>
 __device__ __forceinline__ void hog_user(const DeviceState& s, const EpochParams& p, uint32_t u, float* ring,
                                          int lane) {
     constexpr int AH = ST - 1;
     const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
     const uint32_t slot_f = 2 * Fs + kSlotScalars;  // q row, q^f row, scalars
-    {
-        const uint64_t start = s.user_off[u], end = s.user_off[u + 1];
-        if (start == end) return;
-        const uint64_t n = end - start;
-        const Rec* rr = s.rec + start;
-        const uint64_t ps = s.pr_off[u], pe_ = s.pr_off[u + 1];
-        const uint64_t total = n + (p.full_su ? (pe_ - ps) : 0);
-        const float norm = sqrtf((float)total);
+    Rec* recw = reinterpret_cast<Rec*>(ring + (size_t)ST * slot_f);
+    const uint64_t start = s.user_off[u], end = s.user_off[u + 1];
+    if (start == end) return;
+    const uint64_t n = end - start;
+    const Rec* rr = s.rec + start;
+    const uint64_t ps = s.pr_off[u], pe_ = s.pr_off[u + 1];
+    const uint64_t total = n + (p.full_su ? (pe_ - ps) : 0);
+    const float norm = sqrtf((float)total);
 
-        // ---- su (src/tx.rs:800-822), from the current y
-        float su[VPL], sub = 0.0f;
+    // ---- su (src/tx.rs:800-822), from the current y
+    float su[VPL], sub = 0.0f;
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
-        gather_y8<VPL>(s, n, [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sub);
-        if (p.full_su) {
-            const uint32_t* pp = s.pr_item + ps;
-            gather_y8<VPL>(s, pe_ - ps, [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sub);
-        }
+    for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
+    gather_y8<VPL>(s, n, [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sub);
+    if (p.full_su) {
+        const uint32_t* pp = s.pr_item + ps;
+        gather_y8<VPL>(s, pe_ - ps, [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sub);
+    }
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) su[v] = su[v] / norm;
-        sub = sub / norm;
-        Row<VPL>::store(s.ycache + (size_t)u * Fs, lane, su);
-        if (lane == 0) s.ycache_bias[u] = sub;
+    for (int v = 0; v < VPL; ++v) su[v] = su[v] / norm;
+    sub = sub / norm;
+    Row<VPL>::store(s.ycache + (size_t)u * Fs, lane, su);
+    if (lane == 0) s.ycache_bias[u] = sub;
 
-        float pu[VPL], p2[VPL], seq[VPL];
-        Row<VPL>::load_cg(s.ufeat + (size_t)u * Fs, lane, pu);
-        Row<VPL>::load_cg(s.ufeat2 + (size_t)u * Fs, lane, p2);
+    float pu[VPL], p2[VPL], seq[VPL];
+    Row<VPL>::load_cg(s.ufeat + (size_t)u * Fs, lane, pu);
+    Row<VPL>::load_cg(s.ufeat2 + (size_t)u * Fs, lane, p2);
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) seq[v] = 0.0f;
-        float ub = __ldcg(s.ubias + u), al = __ldcg(s.alpha_u + u), cuu = __ldcg(s.cu + u);
-        float bb0 = lane < (int)T ? __ldcg(s.but_bin + (size_t)u * T + lane) : 0.0f;
-        float bb1 = lane + 32 < (int)T ? __ldcg(s.but_bin + (size_t)u * T + 32 + lane) : 0.0f;
-        float sum_err = 0.0f;
-        const float gb = s.gbias;
+    for (int v = 0; v < VPL; ++v) seq[v] = 0.0f;
+    float ub = __ldcg(s.ubias + u), al = __ldcg(s.alpha_u + u), cuu = __ldcg(s.cu + u);
+    float bb0 = lane < (int)T ? __ldcg(s.but_bin + (size_t)u * T + lane) : 0.0f;
+    float bb1 = lane + 32 < (int)T ? __ldcg(s.but_bin + (size_t)u * T + 32 + lane) : 0.0f;
+    float sum_err = 0.0f;
+    const float gb = s.gbias;
+    const float a_u = 1.0f - p.lr_u * p.reg_u, a_u2 = 1.0f - p.lr_u2 * p.reg_u2;
+    const float k_i = -(p.lr_i * p.reg_i), k_qf = -(p.lr_iqf * p.reg_iqf);
 
-        // record window for the issuer: cur = [w, w+32), nxt = [w+32, w+64)
-        uint64_t w = 0;
-        Rec cur{}, nxt{};
-        if ((uint64_t)lane < n) cur = load_rec(rr + lane);
-        if (32 + (uint64_t)lane < n) nxt = load_rec(rr + 32 + lane);
-        // ubias_day pipeline (lane 0): values and (user, day) indices of ratings t..t+AH
-        float bq[AH + 1];
-        uint32_t dq[AH + 1];
+    // record window: recw[k % kRecWindow] holds record k for k in [wb, wb + kRecWindow)
+    __syncwarp();  // the ring is reused from the previous user
+    for (uint32_t k = lane; k < kRecWindow && k < n; k += 32) recw[k] = load_rec(rr + k);
+    uint64_t wb = 0;
+    __syncwarp();
+    // ubias_day pipeline (lane 0): values and (user, day) indices of ratings t..t+AH
+    float bq[AH + 1];
+    uint32_t dq[AH + 1];
 #pragma unroll
-        for (int a = 0; a <= AH; ++a) {
-            bq[a] = 0.0f;
-            dq[a] = 0xffffffffu;
-        }
-        auto shift = [&]() {
-#pragma unroll
-            for (int a = 0; a < AH; ++a) {
-                bq[a] = bq[a + 1];
-                dq[a] = dq[a + 1];
-            }
-        };
-
-        auto issue = [&](uint64_t t) {
-            if (t >= w + 64) {  // slide the window by one block
-                cur = nxt;
-                w += 32;
-                nxt = Rec{};
-                if (w + 32 + lane < n) nxt = load_rec(rr + w + 32 + lane);
-            }
-            float* slot = ring + (size_t)(t % ST) * slot_f;
-            if (t < n) {
-                const uint32_t o = (uint32_t)(t - w);
-                const Rec ra = shfl_rec(cur, o & 31), rb = shfl_rec(nxt, o & 31);
-                const Rec r = o < 32 ? ra : rb;
-                const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
-                row_cp_async<VPL>(slot, s.ifeat + (size_t)i * Fs, lane);
-                row_cp_async<VPL>(slot + Fs, s.ifeat_freq + (size_t)i * NF * Fs, lane);
-                const bool hud = r.ud < s.n_ud;
-                float* sc = slot + 2 * Fs;
-                if (lane == 0) cp_async4(sc + 0, s.ibias + i);
-                if (lane == 1) cp_async4(sc + 1, s.bit_bin + (size_t)i * T + tb);
-                if (lane == 2) cp_async4(sc + 2, s.ibias_freq + (size_t)i * NF);
-                if (lane == 3) {
-                    if (hud) cp_async4(sc + 3, s.cut + r.ud);
-                    else sc[3] = 0.0f;
-                }
-                if (lane == 4) sc[4] = __uint_as_float(r.key);
-                if (lane == 5) sc[5] = r.res;
-                if (lane == 6) sc[6] = r.dev;
-                if (lane == 7) sc[7] = __uint_as_float(r.ud);
-                if (lane == 8) sc[8] = s.raw ? (float)__ldg(s.raw + (start + t)) : 0.0f;
-                float bnew = 0.0f;
-                if (lane == 0 && hud) bnew = s.ubias_day[r.ud];
-                bq[AH] = bnew;
-                dq[AH] = r.ud;
-            }
-            cp_async_commit();
-        };
-        // prologue: ratings 0..AH-1, shifted into the b/d pipeline
-        __syncwarp();  // the ring is reused from the previous user
+    for (int a = 0; a <= AH; ++a) {
+        bq[a] = 0.0f;
+        dq[a] = 0xffffffffu;
+    }
+    auto shift = [&]() {
 #pragma unroll
         for (int a = 0; a < AH; ++a) {
-            issue((uint64_t)a);
-            shift();
+            bq[a] = bq[a + 1];
+            dq[a] = dq[a + 1];
         }
-        for (uint64_t t = 0; t < n; ++t) {
-            __syncwarp();
-            issue(t + AH);
-            cp_async_wait<AH>();
-            __syncwarp();
-            const float* slot = ring + (size_t)(t % ST) * slot_f;
-            float q[VPL], qf[VPL];
-            row_from_smem<VPL>(slot, lane, q);
-            row_from_smem<VPL>(slot + Fs, lane, qf);
-            const float* sc = slot + 2 * Fs;
-            const float ib = sc[0], bit = sc[1], ibf = sc[2], ct = sc[3];
-            const uint32_t key = __float_as_uint(sc[4]);
-            const float res = sc[5], dv = sc[6];
-            const uint32_t ud = __float_as_uint(sc[7]);
-            const uint32_t i = rec_id(key), tb = rec_tbin(key);
-            const bool hud = ud < s.n_ud;
-            const float bud = __shfl_sync(kFull, bq[0], 0);
-            const float but = __shfl_sync(kFull, tb < 32 ? bb0 : bb1, tb & 31);
-            const float bu_t = ub + but + al * dv + bud + sub;
-            const float bi_t = ib + bit + ibf;
-            const float cu_t = cuu + ct;
-            float part = 0.0f;
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
-            const float dot = warp_sum(part);
-            const float score = gb + bu_t + bi_t * cu_t + dot;
-            // err = score - r, or the ordinal head's d(-log P)/d(score) (src/tx.rs:963-972)
-            float err = score - res;
-            if (s.raw) {  // thresholds are constant while lr_t = 0
-                const float th[4] = {__ldg(s.thresholds), __ldg(s.thresholds + 1), __ldg(s.thresholds + 2),
-                                     __ldg(s.thresholds + 3)};
-                err = ordinal_grad(th, score, (int)sc[8]);
-            }
-            const float err_b = err * p.w_bias, err_d = err * p.w_factor;
-            ub -= p.lr_ub * err_b;
-            {
-                const float nb = but - p.lr_tu * err_b;
-                if (lane == (int)(tb & 31)) {
-                    if (tb < 32) bb0 = nb;
-                    else bb1 = nb;
-                }
-            }
-            al -= p.lr_ta * err_b * dv;
-            if (lane == 0 && hud) {
-                const float nv = bud - p.lr_ubd * err_b;
-                s.ubias_day[ud] = nv;
-#pragma unroll
-                for (int a = 1; a <= AH; ++a)
-                    if (dq[a] == ud) bq[a] = nv;
-            }
-            if (lane == 0) {
-                // item-side updates are applied as atomic deltas: users that
-                // run concurrently never overwrite each other's update
-                atomicAdd(s.ibias + i, -(p.lr_ib * (err_b * cu_t)));
-                atomicAdd(s.bit_bin + (size_t)i * T + tb, -(p.lr_ti * (err_b * cu_t)));
-                atomicAdd(s.ibias_freq + (size_t)i * NF, -(p.lr_ibf * (err_b * cu_t)));
-            }
-            cuu -= p.lr_cu * (err_b * bi_t + p.reg_cu * (cuu - 1.0f));
-            if (!p.sum_err_bug) sum_err += err_b;
-            else
-                for (uint32_t kk = 0; kk < s.F; ++kk) sum_err += err_b;
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) {
-                const float qe = q[v] + qf[v];
-                const float pk = pu[v], p2k = p2[v];
-                seq[v] += err_d * qe;
-                pu[v] = pk - p.lr_u * (err_d * qe + p.reg_u * pk);
-                p2[v] = p2k - p.lr_u2 * (err_d * qe * dv + p.reg_u2 * p2k);
-                const float pe = pk + dv * p2k + 0.0f + su[v];
-                q[v] = -(p.lr_i * (err_d * pe + p.reg_i * q[v]));         // delta of q_i
-                qf[v] = -(p.lr_iqf * (err_d * pe + p.reg_iqf * qf[v]));   // delta of q^f_i
-            }
-            Row<VPL>::red_add(s.ifeat + (size_t)i * Fs, lane, q);
-            Row<VPL>::red_add(s.ifeat_freq + (size_t)i * NF * Fs, lane, qf);
-            shift();
-        }
-        cp_async_wait<0>();
+    };
 
-        Row<VPL>::store(s.ufeat + (size_t)u * Fs, lane, pu);
-        Row<VPL>::store(s.ufeat2 + (size_t)u * Fs, lane, p2);
+    auto issue = [&](uint64_t t) {
+        if (t < n) {
+            if (t == wb + kRecWindow) {
+                // records t .. t+31 replace wb .. wb+31, all consumed by now
+                __syncwarp();
+                if (t + lane < n) recw[(t + lane) % kRecWindow] = load_rec(rr + t + lane);
+                wb += 32;
+                __syncwarp();
+            }
+            const Rec r = recw[t % kRecWindow];
+            const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+            const bool hud = r.ud < s.n_ud;
+            float* slot = ring + (size_t)(t % ST) * slot_f;
+            row_cp_async<VPL>(slot, s.ifeat + (size_t)i * Fs, lane);
+            row_cp_async<VPL>(slot + Fs, s.ifeat_freq + (size_t)i * NF * Fs, lane);
+            if (lane < 4) {
+                const float* src = lane == 0   ? s.ibias + i
+                                   : lane == 1 ? s.bit_bin + (size_t)i * T + tb
+                                   : lane == 2 ? s.ibias_freq + (size_t)i * NF
+                                               : s.cut + (hud ? r.ud : 0u);
+                cp_async4(slot + 2 * Fs + lane, src);
+            }
+            float bnew = 0.0f;
+            if (lane == 0 && hud) bnew = s.ubias_day[r.ud];
+            bq[AH] = bnew;
+            dq[AH] = r.ud;
+        }
+        cp_async_commit();
+    };
+    // prologue: ratings 0..AH-1, shifted into the b/d pipeline
+#pragma unroll
+    for (int a = 0; a < AH; ++a) {
+        issue((uint64_t)a);
+        shift();
+    }
+    for (uint64_t t = 0; t < n; ++t) {
+        __syncwarp();
+        issue(t + AH);
+        cp_async_wait<AH>();
+        __syncwarp();
+        const float* slot = ring + (size_t)(t % ST) * slot_f;
+        float q[VPL], qf[VPL];
+        row_from_smem<VPL>(slot, lane, q);
+        row_from_smem<VPL>(slot + Fs, lane, qf);
+        const float4 scv = *reinterpret_cast<const float4*>(slot + 2 * Fs);
+        const Rec r = recw[t % kRecWindow];
+        const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+        const uint32_t ud = r.ud;
+        const bool hud = ud < s.n_ud;
+        const float dv = r.dev;
+        const float ib = scv.x, bit = scv.y, ibf = scv.z, ct = hud ? scv.w : 0.0f;
+        const float bud = __shfl_sync(kFull, bq[0], 0);
+        const float but = __shfl_sync(kFull, tb < 32 ? bb0 : bb1, tb & 31);
+        const float bu_t = ub + but + al * dv + bud + sub;
+        const float bi_t = ib + bit + ibf;
+        const float cu_t = cuu + ct;
+        float part = 0.0f;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
+        const float dot = warp_sum(part);
+        const float score = gb + bu_t + bi_t * cu_t + dot;
+        // err = score - r, or the ordinal head's d(-log P)/d(score) (src/tx.rs:963-972)
+        float err = score - r.res;
+        if (s.raw) {  // thresholds are constant while lr_t = 0
+            const float th[4] = {__ldg(s.thresholds), __ldg(s.thresholds + 1), __ldg(s.thresholds + 2),
+                                 __ldg(s.thresholds + 3)};
+            err = ordinal_grad(th, score, (int)__ldg(s.raw + start + t));
+        }
+        const float err_b = err * p.w_bias, err_d = err * p.w_factor;
+        ub -= p.lr_ub * err_b;
+        {
+            const float nb = but - p.lr_tu * err_b;
+            if (lane == (int)(tb & 31)) {
+                if (tb < 32) bb0 = nb;
+                else bb1 = nb;
+            }
+        }
+        al -= p.lr_ta * err_b * dv;
+        if (lane == 0 && hud) {
+            const float nv = bud - p.lr_ubd * err_b;
+            s.ubias_day[ud] = nv;
+#pragma unroll
+            for (int a = 1; a <= AH; ++a)
+                if (dq[a] == ud) bq[a] = nv;
+        }
         if (lane == 0) {
-            s.ubias[u] = ub;
-            s.alpha_u[u] = al;
-            s.cu[u] = cuu;
+            // item-side updates are applied as atomic deltas: users that
+            // run concurrently never overwrite each other's update
+            const float ge = err_b * cu_t;
+            atomicAdd(s.ibias + i, -(p.lr_ib * ge));
+            atomicAdd(s.bit_bin + (size_t)i * T + tb, -(p.lr_ti * ge));
+            atomicAdd(s.ibias_freq + (size_t)i * NF, -(p.lr_ibf * ge));
         }
-        if (lane < (int)T) s.but_bin[(size_t)u * T + lane] = bb0;
-        if (lane + 32 < (int)T) s.but_bin[(size_t)u * T + 32 + lane] = bb1;
+        cuu -= p.lr_cu * (err_b * bi_t + p.reg_cu * (cuu - 1.0f));
+        if (!p.sum_err_bug) sum_err += err_b;
+        else
+            for (uint32_t kk = 0; kk < s.F; ++kk) sum_err += err_b;
+        const float nlu = -(p.lr_u * err_d), nlu2 = -(p.lr_u2 * err_d) * dv;
+        const float nli = -(p.lr_i * err_d), nlf = -(p.lr_iqf * err_d);
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+            const float qe = q[v] + qf[v];
+            const float pk = pu[v], p2k = p2[v];
+            seq[v] += err_d * qe;
+            pu[v] = fmaf(nlu, qe, a_u * pk);
+            p2[v] = fmaf(nlu2, qe, a_u2 * p2k);
+            const float pe = fmaf(dv, p2k, pk) + su[v];
+            q[v] = fmaf(nli, pe, k_i * q[v]);     // delta of q_i
+            qf[v] = fmaf(nlf, pe, k_qf * qf[v]);  // delta of q^f_i
+        }
+        Row<VPL>::red_add(s.ifeat + (size_t)i * Fs, lane, q);
+        Row<VPL>::red_add(s.ifeat_freq + (size_t)i * NF * Fs, lane, qf);
+        shift();
+    }
+    cp_async_wait<0>();
 
-        // ---- NSVD1 factor & bias updates at the end of the user (src/tx.rs:1099-1106)
-        float g[VPL];
+    Row<VPL>::store(s.ufeat + (size_t)u * Fs, lane, pu);
+    Row<VPL>::store(s.ufeat2 + (size_t)u * Fs, lane, p2);
+    if (lane == 0) {
+        s.ubias[u] = ub;
+        s.alpha_u[u] = al;
+        s.cu[u] = cuu;
+    }
+    if (lane < (int)T) s.but_bin[(size_t)u * T + lane] = bb0;
+    if (lane + 32 < (int)T) s.but_bin[(size_t)u * T + 32 + lane] = bb1;
+
+    // ---- NSVD1 factor & bias updates at the end of the user (src/tx.rs:1099-1106)
+    float g[VPL];
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) g[v] = seq[v] / norm;
-        const float eb = sum_err / norm;
-        for (uint64_t base = 0; base < n; base += 32) {
-            const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
-            const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&rr[base + lane].key)) : 0u;
-            for (uint32_t j = 0; j < cnt; j += kBatch) {
-                float y[kBatch][VPL];
-                uint32_t its[kBatch];
+    for (int v = 0; v < VPL; ++v) g[v] = seq[v] / norm;
+    const float eb = sum_err / norm;
+    for (uint64_t base = 0; base < n; base += 32) {
+        const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
+        const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&rr[base + lane].key)) : 0u;
+        for (uint32_t j = 0; j < cnt; j += kBatch) {
+            float y[kBatch][VPL];
+            uint32_t its[kBatch];
 #pragma unroll
-                for (int q = 0; q < kBatch; ++q) {
-                    its[q] = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
-                    Row<VPL>::load_cg(s.yfeat + (size_t)its[q] * Fs, lane, y[q]);
-                }
+            for (int b = 0; b < kBatch; ++b) {
+                its[b] = __shfl_sync(kFull, mine, j + b < cnt ? j + b : cnt - 1);
+                Row<VPL>::load_cg(s.yfeat + (size_t)its[b] * Fs, lane, y[b]);
+            }
 #pragma unroll
-                for (int q = 0; q < kBatch; ++q) {
-                    if (j + q < cnt) {
+            for (int b = 0; b < kBatch; ++b) {
+                if (j + b < cnt) {
 #pragma unroll
-                        for (int v = 0; v < VPL; ++v) y[q][v] = -(p.lr_y * (g[v] + p.reg_y * y[q][v]));
-                        Row<VPL>::red_add(s.yfeat + (size_t)its[q] * Fs, lane, y[q]);
-                        if (lane == 0) atomicAdd(s.ybias + its[q], -(p.lr_yb * eb));
-                    }
+                    for (int v = 0; v < VPL; ++v) y[b][v] = -(p.lr_y * (g[v] + p.reg_y * y[b][v]));
+                    Row<VPL>::red_add(s.yfeat + (size_t)its[b] * Fs, lane, y[b]);
+                    if (lane == 0) atomicAdd(s.ybias + its[b], -(p.lr_yb * eb));
                 }
             }
         }
@@ -289,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_hog_pass(DeviceState s, EpochPa
                                                           const uint32_t* __restrict__ order, uint32_t n_work) {
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float* ring = smem + (size_t)warp * kStages * (2 * s.Fs + kSlotScalars);
+    float* ring = smem + (size_t)warp * hog_ring_floats(kStages, s.Fs);
     for (;;) {
         uint32_t k = 0;
         if (lane == 0) k = atomicAdd(&s.counters[0], 1u);
@@ -449,7 +451,7 @@ __device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bf
 // ---------------------------------------------------------------------------
 template <int VPL>
 void launch_hog_pass(tsvd_model* m, const EpochParams& p, const uint32_t* order) {
-    const size_t smem = (size_t)kWarps * kStages * (2 * m->d.Fs + kSlotScalars) * sizeof(float);
+    const size_t smem = (size_t)kWarps * hog_ring_floats(kStages, m->d.Fs) * sizeof(float);
     TSVD_CUDA(cudaFuncSetAttribute(k_hog_pass<VPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     unsigned g = persistent_grid(k_hog_pass<VPL>, smem);
     k_hog_pass<VPL><<<g, kThreads, smem, m->stream>>>(m->d, p, order, m->d.n_users);

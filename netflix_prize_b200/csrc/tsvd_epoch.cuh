@@ -9,9 +9,16 @@ namespace tsvd {
 
 constexpr int kWarps = 8;  // warps per block
 constexpr int kThreads = kWarps * 32;
-// Hogwild ring slot: q row, q^f row, then kSlotScalars floats of per-rating
-// scalars (a multiple of 4, so every row stays 16-byte aligned).
-constexpr uint32_t kSlotScalars = 12;
+// Hogwild ring slot: q row, q^f row, then kSlotScalars floats of item-side
+// scalars (a multiple of 4, so every row stays 16-byte aligned). After the
+// slots, a window of kRecWindow rating records (16 bytes each).
+constexpr uint32_t kSlotScalars = 4;
+constexpr uint32_t kRecWindow = 64;
+
+// Shared-memory floats of one warp's Hogwild ring with `st` slots.
+__host__ __device__ __forceinline__ uint32_t hog_ring_floats(int st, uint32_t Fs) {
+    return (uint32_t)st * (2 * Fs + kSlotScalars) + kRecWindow * 4;
+}
 
 struct EpochParams {
     float lr_u, lr_u2, lr_ub, lr_ubd, lr_i, lr_ib, lr_y, lr_yb, lr_tu, lr_ti, lr_ta, lr_ibf, lr_iqf, lr_cu;

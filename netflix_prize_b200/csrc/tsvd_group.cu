@@ -95,7 +95,7 @@ uint32_t ring_floats_for(const std::vector<tsvd_model*>& ms) {
     uint32_t r = 0;
     for (auto* m : ms) {
         const uint32_t st = tsvd::make_params(m).stages;
-        r = std::max<uint32_t>(r, st * (2 * m->d.Fs + tsvd::kSlotScalars));
+        r = std::max<uint32_t>(r, tsvd::hog_ring_floats(st, m->d.Fs));
     }
     return r;
 }
@@ -337,7 +337,7 @@ int tsvd_group_autotune(tsvd_group* g, uint32_t sample_users, int32_t* chosen_st
                     TSVD_CUDA(cudaEventRecord(e0, g->stream));
                     tsvd::launch_hog_batched(g->stream, st_buf.as<tsvd::DeviceState>(),
                                              pa_buf.as<tsvd::EpochParams>(), un_buf.as<uint32_t>(), ns,
-                                             (uint32_t)stages * (2 * tmp->d.Fs + tsvd::kSlotScalars),
+                                             tsvd::hog_ring_floats(stages, tmp->d.Fs),
                                              cnt_buf.as<uint32_t>());
                     TSVD_CUDA(cudaEventRecord(e1, g->stream));
                     TSVD_CUDA(cudaStreamSynchronize(g->stream));
@@ -359,7 +359,7 @@ int tsvd_group_autotune(tsvd_group* g, uint32_t sample_users, int32_t* chosen_st
         }
         g->ring_floats = 0;
         for (auto* m : g->models)
-            g->ring_floats = std::max<uint32_t>(g->ring_floats, m->stages * (2 * m->d.Fs + tsvd::kSlotScalars));
+            g->ring_floats = std::max<uint32_t>(g->ring_floats, tsvd::hog_ring_floats(m->stages, m->d.Fs));
         if (g->exec) {  // the captured graph baked in the old ring size
             cudaGraphExecDestroy(g->exec);
             cudaGraphDestroy(g->graph);

@@ -299,7 +299,8 @@ int tsvd_encoder_forward(tsvd_encoder* e, const uint32_t* users, uint32_t n, flo
 /* Writes de-standardised predictions of p_u, b_u, alpha_u into model m for
  * `users` and resets their other user state to the standard init. */
 int tsvd_encoder_apply(tsvd_encoder* e, tsvd_model* m, const uint32_t* users, uint64_t n);
-/* Parameters (or gradients as "g.<name>"): e_item, e_rate, e_date, w1, b1,
+/* Parameters (or gradients as "g.<name>"): e_item [n_items * 5, 128] (row
+ * 5 i + r - 1 for item i rated r), e_rate [5, 128], e_date [T, 128], w1, b1,
  * w2, b2, w3, b3; FP32, matrices [in, out] row-major. */
 int tsvd_encoder_get(const tsvd_encoder* e, const char* name, float* dst, uint64_t count);
 int tsvd_encoder_set(tsvd_encoder* e, const char* name, const float* src, uint64_t count);

@@ -5,8 +5,10 @@
 // itself is the reference's user-side SGD with item tables frozen
 // (src/tsvdx4p.rs:390-639).
 //
-//   h0 = mean over the user's training ratings of
-//        E_item[i] + E_rating[r - 1] + E_date[time_bin(t)]          (dim 128)
+//   h0 = mean over the user's training ratings (i, r, t) of
+//        E_item[i, r] + E_rating[r - 1] + E_date[time_bin(t)]       (dim 128)
+// E_item has one row per (item, rating) pair, so h0 carries which items the
+// user rated how, not only which items and which ratings.
 //   h1 = GELU(h0 W1 + b1)   128 -> 512
 //   h2 = GELU(h1 W2 + b2)   512 -> 512
 //   y  = h2 W3 + b3         512 -> f + 2   (standardised p_u, b_u, alpha_u)
@@ -174,17 +176,37 @@ __global__ void __launch_bounds__(256) k_embag_fwd(DeviceState s, const int8_t* 
     const uint32_t u = users[w];
     const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (uint64_t t = a; t < b; ++t) {
-        const Rec r = load_rec(s.rec + t);
-        const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
-        const int rt = min(max((int)raw[t], 1), 5) - 1;
-        const float4 x = __ldg(reinterpret_cast<const float4*>(e_item + (size_t)i * kEmb) + lane);
-        const float4 y = __ldg(reinterpret_cast<const float4*>(e_rate + (size_t)rt * kEmb) + lane);
-        const float4 z = __ldg(reinterpret_cast<const float4*>(e_date + (size_t)tb * kEmb) + lane);
-        acc.x += x.x + y.x + z.x;
-        acc.y += x.y + y.y + z.y;
-        acc.z += x.z + y.z + z.z;
-        acc.w += x.w + y.w + z.w;
+    for (uint64_t base = a; base < b; base += 32) {
+        // one record per lane, then four rows in flight per step
+        const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+        uint32_t row = 0, tbv = 0, rtv = 0;
+        if ((uint32_t)lane < cnt) {
+            const Rec r = load_rec(s.rec + base + lane);
+            rtv = (uint32_t)(min(max((int)raw[base + lane], 1), 5) - 1);
+            row = rec_id(r.key) * 5u + rtv;
+            tbv = rec_tbin(r.key);
+        }
+        for (uint32_t j = 0; j < cnt; j += 4) {
+            float4 x[4], y[4], z[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int src = (int)(j + q < cnt ? j + q : j);
+                const uint32_t ro = __shfl_sync(kFull, row, src), tq = __shfl_sync(kFull, tbv, src),
+                               rq = __shfl_sync(kFull, rtv, src);
+                x[q] = __ldg(reinterpret_cast<const float4*>(e_item + (size_t)ro * kEmb) + lane);
+                y[q] = __ldg(reinterpret_cast<const float4*>(e_rate + (size_t)rq * kEmb) + lane);
+                z[q] = __ldg(reinterpret_cast<const float4*>(e_date + (size_t)tq * kEmb) + lane);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (j + q < cnt) {
+                    acc.x += x[q].x + y[q].x + z[q].x;
+                    acc.y += x[q].y + y[q].y + z[q].y;
+                    acc.z += x[q].z + y[q].z + z[q].z;
+                    acc.w += x[q].w + y[q].w + z[q].w;
+                }
+            }
+        }
     }
     const float inv = b > a ? 1.0f / (float)(b - a) : 0.0f;
     acc.x *= inv; acc.y *= inv; acc.z *= inv; acc.w *= inv;
@@ -194,37 +216,60 @@ __global__ void __launch_bounds__(256) k_embag_fwd(DeviceState s, const int8_t* 
     o[2] = __float2bfloat16(acc.z); o[3] = __float2bfloat16(acc.w);
 }
 
-// dE += dh0 / n_u for every rating of every user in the batch (atomics: users
-// share items).
+// dE += dh0 / n_u for every rating of every user in the batch: vector atomics
+// into the (item, rating) rows, which users share; the few date-bin rows that
+// every rating hits are summed per block in shared memory first.
 __global__ void __launch_bounds__(256) k_embag_bwd(DeviceState s, const int8_t* __restrict__ raw,
                                                    const uint32_t* __restrict__ users, int n,
                                                    const float* __restrict__ dh0, float* __restrict__ g_item,
                                                    float* __restrict__ g_rate, float* __restrict__ g_date) {
+    __shared__ float sdate[kMaxBins * kEmb];  // T <= kMaxBins date rows
     const int lane = threadIdx.x & 31;
+    const uint32_t T = s.T;
+    for (uint32_t k = threadIdx.x; k < T * kEmb; k += blockDim.x) sdate[k] = 0.0f;
+    __syncthreads();
     const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (w >= n) return;
-    const uint32_t u = users[w];
-    const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
-    if (a == b) return;
-    const float inv = 1.0f / (float)(b - a);
-    float4 d = reinterpret_cast<const float4*>(dh0 + (size_t)w * kEmb)[lane];
-    d.x *= inv; d.y *= inv; d.z *= inv; d.w *= inv;
-    float4 rs[5];
-    for (int q = 0; q < 5; ++q) rs[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (uint64_t t = a; t < b; ++t) {
-        const Rec r = load_rec(s.rec + t);
-        const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
-        const int rt = min(max((int)raw[t], 1), 5) - 1;
-        float* gi = g_item + (size_t)i * kEmb + 4 * lane;
-        atomicAdd(gi, d.x); atomicAdd(gi + 1, d.y); atomicAdd(gi + 2, d.z); atomicAdd(gi + 3, d.w);
-        float* gd = g_date + (size_t)tb * kEmb + 4 * lane;
-        atomicAdd(gd, d.x); atomicAdd(gd + 1, d.y); atomicAdd(gd + 2, d.z); atomicAdd(gd + 3, d.w);
-        rs[rt].x += d.x; rs[rt].y += d.y; rs[rt].z += d.z; rs[rt].w += d.w;
+    const uint32_t u = w < n ? users[w] : 0u;
+    const uint64_t a = w < n ? s.user_off[u] : 0, b = w < n ? s.user_off[u + 1] : 0;
+    if (b > a) {
+        const float inv = 1.0f / (float)(b - a);
+        float4 d = reinterpret_cast<const float4*>(dh0 + (size_t)w * kEmb)[lane];
+        d.x *= inv; d.y *= inv; d.z *= inv; d.w *= inv;
+        float4 rs[5];
+        for (int q = 0; q < 5; ++q) rs[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint64_t base = a; base < b; base += 32) {
+            const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+            uint32_t row = 0, tbv = 0, rtv = 0;
+            if ((uint32_t)lane < cnt) {
+                const Rec r = load_rec(s.rec + base + lane);
+                rtv = (uint32_t)(min(max((int)raw[base + lane], 1), 5) - 1);
+                row = rec_id(r.key) * 5u + rtv;
+                tbv = rec_tbin(r.key);
+            }
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const uint32_t ro = __shfl_sync(kFull, row, (int)j), tb = __shfl_sync(kFull, tbv, (int)j),
+                               rt = __shfl_sync(kFull, rtv, (int)j);
+                float* gi = g_item + (size_t)ro * kEmb + 4 * lane;
+                asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(gi), "f"(d.x), "f"(d.y),
+                             "f"(d.z), "f"(d.w)
+                             : "memory");
+                float* sd = sdate + tb * kEmb + 4 * lane;
+                atomicAdd(sd, d.x); atomicAdd(sd + 1, d.y); atomicAdd(sd + 2, d.z); atomicAdd(sd + 3, d.w);
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+                    if ((int)rt == q) {
+                        rs[q].x += d.x; rs[q].y += d.y; rs[q].z += d.z; rs[q].w += d.w;
+                    }
+            }
+        }
+        for (int q = 0; q < 5; ++q) {
+            float* gr = g_rate + (size_t)q * kEmb + 4 * lane;
+            atomicAdd(gr, rs[q].x); atomicAdd(gr + 1, rs[q].y); atomicAdd(gr + 2, rs[q].z); atomicAdd(gr + 3, rs[q].w);
+        }
     }
-    for (int q = 0; q < 5; ++q) {
-        float* gr = g_rate + (size_t)q * kEmb + 4 * lane;
-        atomicAdd(gr, rs[q].x); atomicAdd(gr + 1, rs[q].y); atomicAdd(gr + 2, rs[q].z); atomicAdd(gr + 3, rs[q].w);
-    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < T * kEmb; k += blockDim.x)
+        if (sdate[k] != 0.0f) atomicAdd(g_date + k, sdate[k]);
 }
 
 // Standardised targets of a batch: [p_u (f), b_u, alpha_u].
@@ -508,7 +553,14 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
             e->params.push_back(std::move(p));
         };
         const int O = e->O;
-        add("e_item", (size_t)s.n_items * kEmb, false, false, 0.05f, false);
+        // (item, rating) rows, N(0, 0.05) drawn on the device from a stream of their own
+        add("e_item", (size_t)s.n_items * 5 * kEmb, false, false, 0.0f, false);
+        {
+            const NormalTable t{e->params.back().w.as<float>(), (uint64_t)s.n_items * 5, (uint32_t)kEmb,
+                                (uint32_t)kEmb, 0.05f};
+            device_normal_tables(&t, 1, seed ^ 0x5eed5eed5eed5eedull, e->stream);
+            TSVD_CUDA(cudaStreamSynchronize(e->stream));
+        }
         add("e_rate", 5 * kEmb, false, false, 0.05f, false);
         add("e_date", (size_t)s.T * kEmb, false, false, 0.05f, false);
         add("w1", (size_t)kEmb * kHid, true, true, std::sqrt(6.0f / (kEmb + kHid)), true);

@@ -73,7 +73,7 @@ class UserEncoder:
 
     def shape(self, name: str):
         base = name[2:] if name.startswith("g.") else name
-        return {"e_item": (self.n_items, 128), "e_rate": (5, 128), "e_date": (self.T, 128), "w1": (128, 512),
+        return {"e_item": (self.n_items * 5, 128), "e_rate": (5, 128), "e_date": (self.T, 128), "w1": (128, 512),
                 "b1": (512,), "w2": (512, 512), "b2": (512,), "w3": (512, self.O), "b3": (self.O,)}[base]
 
     def get(self, name: str) -> np.ndarray:

@@ -2,7 +2,8 @@
 gradients, used to check the GPU's forward/backward kernels.
 
 The encoder has no counterpart in the reference. Its definition:
-  h0 = mean over the user's training ratings of E_item[i] + E_rate[r-1] + E_date[b]
+  h0 = mean over the user's training ratings of E_item[5 i + r - 1] + E_rate[r-1] + E_date[b]
+  (E_item has one row per (item, rating) pair)
   z1 = h0 W1 + b1, h1 = GELU(z1); z2 = h1 W2 + b2, h2 = GELU(z2); y = h2 W3 + b3
   loss = mean((y - t)^2) over the batch and the f+2 outputs, t standardised.
 With mimic_bf16 the oracle rounds to BF16 exactly where the GPU stores BF16
@@ -42,7 +43,7 @@ def loss_and_grads(params, hist, targets, mimic_bf16=True):
     h0 = np.zeros((n, 128))
     for k, (it, rt, tb) in enumerate(hist):
         if len(it):
-            h0[k] = (P["e_item"][it] + P["e_rate"][rt - 1] + P["e_date"][tb]).sum(0) / len(it)
+            h0[k] = (P["e_item"][5 * it + rt - 1] + P["e_rate"][rt - 1] + P["e_date"][tb]).sum(0) / len(it)
     if mimic_bf16:  # the GPU accumulates h0 in FP32 and stores that value
         h0 = h0.astype(np.float32).astype(np.float64)
     W1, W2, W3 = r(P["w1"]), r(P["w2"]), r(P["w3"])
@@ -77,7 +78,7 @@ def loss_and_grads(params, hist, targets, mimic_bf16=True):
         if not len(it):
             continue
         dk = dh0[k] / len(it)
-        np.add.at(ge_item, it, dk)
+        np.add.at(ge_item, 5 * it + rt - 1, dk)
         np.add.at(ge_rate, rt - 1, dk)
         np.add.at(ge_date, tb, dk)
     g["e_item"], g["e_rate"], g["e_date"] = ge_item, ge_rate, ge_date

@@ -7,7 +7,7 @@ from oracle import encoder_oracle as eo
 
 def small_problem(seed=0, n_items=12, T=5, O=6, n_users=4):
     rng = np.random.default_rng(seed)
-    p = {"e_item": rng.normal(0, 0.3, (n_items, 128)), "e_rate": rng.normal(0, 0.3, (5, 128)),
+    p = {"e_item": rng.normal(0, 0.3, (n_items * 5, 128)), "e_rate": rng.normal(0, 0.3, (5, 128)),
          "e_date": rng.normal(0, 0.3, (T, 128)), "w1": rng.normal(0, 0.1, (128, 512)),
          "b1": rng.normal(0, 0.1, 512), "w2": rng.normal(0, 0.05, (512, 512)), "b2": rng.normal(0, 0.1, 512),
          "w3": rng.normal(0, 0.05, (512, O)), "b3": rng.normal(0, 0.1, O)}
@@ -27,7 +27,7 @@ def test_oracle_gradients_match_finite_differences():
     for name in ("e_item", "e_rate", "e_date", "w1", "b1", "w2", "b2", "w3", "b3"):
         for _ in range(4):
             idx = tuple(rng.integers(0, s) for s in p[name].shape)
-            if name == "e_item" and not any(idx[0] in it for it, _, _ in hist):
+            if name == "e_item" and not any(idx[0] in 5 * it + rt - 1 for it, rt, _ in hist):
                 continue
             q = {k: v.copy() for k, v in p.items()}
             q[name][idx] += h

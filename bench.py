@@ -47,20 +47,30 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--f", type=int, default=256)
     ap.add_argument("--shape", choices=["c2", "c1", "c3"], default="c2")
-    ap.add_argument("--schedule", choices=["hogwild", "stratified"], default="hogwild")
+    ap.add_argument("--schedule", choices=["hogwild", "stratified"], default="stratified")
     ap.add_argument("--precision", choices=["fp32", "bf16", "bf16all"], default="fp32",
                     help="BF16 read copies (stratified only): item and y tables, or also user rows")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ttr", action="store_true", help="skip the fold-in time-to-RMSE comparison")
     ap.add_argument("--sample-users", type=int, default=20000, help="users in the CPU sample")
     return ap.parse_args()
 
 
 def B_per_rating(f: int) -> int:
-    """Algorithmic bytes per rating-update, low_memory tx4 mode: q_i and
-    q^f_i read+write (16 f), y_j gather (4 f) and read-modify-write (8 f),
-    64 bytes of stream and bias scalars."""
+    """Algorithmic bytes per rating-update of the per-user pass, low_memory
+    tx4 mode: q_i and q^f_i read+write (16 f), y_j gather (4 f) and
+    read-modify-write (8 f), 64 bytes of stream and bias scalars."""
     return 28 * f + 64
+
+
+def kernel_bytes_per_rating(kernel: str, f: int) -> int:
+    """Algorithmic bytes per rating of the kernel the roofline is quoted on."""
+    if kernel == "item_pass":
+        # item stratum: the rating's user rows p, p2, ycache (12 f), its 16-byte
+        # record and 7 user-side bias scalars; item rows stay on chip per item
+        return 12 * f + 44
+    return B_per_rating(f)
 
 
 def spec_for(shape: str):
@@ -222,6 +232,64 @@ def cpu_baseline(args):
                       f"{args.shape} generator, f={args.f}; host has {os.cpu_count()} cores"}
 
 
+def time_to_rmse(model, tr, pr):
+    """Time to a held-out RMSE target for new users (the C5 fold-in): the
+    plain form (standard init + user-side SGD passes with item tables frozen)
+    against the chosen form (encoder init + passes). The model's other
+    480,189 - 80,189 users (same proportion at other shapes) train the
+    encoder for 10 epochs; the 80,189 are reset and folded in. Target =
+    plain RMSE after 8 passes + 0.001. Times are host wall clock around the
+    synchronous C ABI calls."""
+    import numpy as np
+    from netflix_prize_b200.data import Dataset
+    from netflix_prize_b200.encoder import UserEncoder, foldin, reset_users
+
+    U = tr.n_users
+    n_new = max(1, U - int(round(U * 400000 / 480189)))
+    perm = np.random.default_rng(0).permutation(U).astype(np.uint32)
+    new, old = np.sort(perm[:n_new]), perm[n_new:]
+    keep = np.isin(pr.user_idxs, new) & (pr.is_test == 0)
+    held = Dataset.from_ratings(pr.user_idxs[keep], pr.item_idxs[keep], pr.raw_ratings[keep], pr.dates[keep],
+                                pr.n_users, pr.n_items, "held_new_users")
+    model.synchronize()
+    t0 = time.perf_counter()
+    enc = UserEncoder(model, tr.raw_ratings, old, seed=5, lr=2e-3)
+    losses = [enc.train_epoch(old, batch=1024) for _ in range(10)]
+    model.synchronize()
+    enc_s = time.perf_counter() - t0
+
+    def run(k, warm):
+        reset_users(model, new, 99)
+        model.synchronize()
+        t = time.perf_counter()
+        if warm:
+            enc.apply(model, new)
+        if k:
+            foldin(model, new, k)
+        model.synchronize()
+        return (time.perf_counter() - t) * 1000.0, model.calc_rmse(held)
+
+    plain = [(k,) + run(k, False) for k in range(0, 9)]
+    target = plain[-1][2] + 0.001
+    warm = []
+    for k in range(0, 5):
+        warm.append((k,) + run(k, True))
+        if warm[-1][2] <= target:
+            break
+    first = lambda rows: next((r for r in rows if r[2] <= target), None)
+    p, w = first(plain), first(warm)
+    enc.close()
+    return {"scenario": f"fold-in of {n_new} held-out users of the trained model, item tables frozen",
+            "target_rmse": target, "target_rule": "plain RMSE after 8 passes + 0.001",
+            "plain": {"passes": p[0], "ms": p[1], "rmse": p[2]} if p else None,
+            "chosen": {"form": "encoder init + fold-in passes", "passes": w[0], "ms": w[1], "rmse": w[2]}
+            if w else None,
+            "chosen_over_plain_time": (w[1] / p[1]) if (p and w and p[1] > 0) else None,
+            "encoder_train_s": enc_s, "encoder_loss_first_last": [losses[0], losses[-1]],
+            "plain_curve": [[k, round(ms, 3), r] for k, ms, r in plain],
+            "chosen_curve": [[k, round(ms, 3), r] for k, ms, r in warm]}
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -293,9 +361,13 @@ def main():
     value = R * args.steps * world / (ms / 1000.0)
     peak, peak_kind = measured_peaks()
     dom = kstats.get(kname, {"avg_ms": float("nan")})
-    achieved = B_per_rating(args.f) * R / (dom["avg_ms"] / 1000.0) / 1e9
+    bpr = kernel_bytes_per_rating(kname, args.f)
+    achieved = bpr * R / (dom["avg_ms"] / 1000.0) / 1e9
     workload = f"{args.shape}_f{args.f}_{args.schedule}"
     traffic = traffic_record(kname, workload)
+    ttr = None
+    if world == 1 and not args.no_ttr:
+        ttr = time_to_rmse(model, tr, pr)
     del model
 
     # ---------------- e2e: through the C ABI from pinned host buffers ----------------
@@ -343,12 +415,13 @@ def main():
         "config": workload_config(args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": kname,
-                     "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_rating": B_per_rating(args.f)},
+                     "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_rating": bpr},
         "kernels": kstats,
         "heldout_rmse_after_run": rmse,
         "clocks": clk,
         "gpu_launches": launches,
         "e2e": e2e,
+        "time_to_rmse": ttr,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)

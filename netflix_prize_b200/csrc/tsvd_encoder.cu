@@ -162,114 +162,138 @@ void gemm(cudaStream_t st, const __nv_bfloat16* A, int a_km, int lda, const __nv
 }
 
 // ---------------------------------------------------------------------------
-// Embedding bag over a batch of users: warp per user, 4 of the 128 dims per
-// lane. Emits FP32 and BF16 copies of h0.
+// Embedding bag over a batch of users, one block per user: the 8 warps take
+// the user's 32-rating chunks in turn (8 rows in flight per warp) and sum the
+// (item, rating) rows; the rating and date-bin rows enter through the user's
+// histograms, hist[w] = {counts of ratings 1..5, counts of date bins}, which
+// the block also writes for the backward pass. Partial sums are combined in
+// warp order, so results do not depend on scheduling.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_embag_fwd(DeviceState s, const int8_t* __restrict__ raw,
-                                                   const uint32_t* __restrict__ users, int n,
-                                                   const float* __restrict__ e_item, const float* __restrict__ e_rate,
-                                                   const float* __restrict__ e_date, float* __restrict__ h0,
-                                                   __nv_bfloat16* __restrict__ h0b) {
-    const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (w >= n) return;
+constexpr int kBagWarps = 8;
+
+__global__ void __launch_bounds__(kBagWarps * 32) k_embag_fwd(DeviceState s, const int8_t* __restrict__ raw,
+                                                            const uint32_t* __restrict__ users, int n,
+                                                            const float* __restrict__ e_item,
+                                                            const float* __restrict__ e_rate,
+                                                            const float* __restrict__ e_date, float* __restrict__ h0,
+                                                            __nv_bfloat16* __restrict__ h0b, float* __restrict__ hist,
+                                                            float* __restrict__ inv_n) {
+    __shared__ float4 part[kBagWarps][32];
+    __shared__ int cnt_sh[5 + kMaxBins];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int w = blockIdx.x;
+    const uint32_t T = s.T, H = 5 + T;
+    for (uint32_t k = threadIdx.x; k < H; k += blockDim.x) cnt_sh[k] = 0;
+    __syncthreads();
     const uint32_t u = users[w];
     const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (uint64_t base = a; base < b; base += 32) {
-        // one record per lane, then four rows in flight per step
+    for (uint64_t base = a + (uint64_t)warp * 32; base < b; base += (uint64_t)kBagWarps * 32) {
         const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
-        uint32_t row = 0, tbv = 0, rtv = 0;
+        uint32_t row = 0;
         if ((uint32_t)lane < cnt) {
             const Rec r = load_rec(s.rec + base + lane);
-            rtv = (uint32_t)(min(max((int)raw[base + lane], 1), 5) - 1);
-            row = rec_id(r.key) * 5u + rtv;
-            tbv = rec_tbin(r.key);
+            const int rt = min(max((int)raw[base + lane], 1), 5) - 1;
+            row = rec_id(r.key) * 5u + (uint32_t)rt;
+            atomicAdd(&cnt_sh[rt], 1);
+            atomicAdd(&cnt_sh[5 + rec_tbin(r.key)], 1);
         }
-        for (uint32_t j = 0; j < cnt; j += 4) {
-            float4 x[4], y[4], z[4];
+        for (uint32_t j = 0; j < cnt; j += 8) {
+            float4 x[8];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int src = (int)(j + q < cnt ? j + q : j);
-                const uint32_t ro = __shfl_sync(kFull, row, src), tq = __shfl_sync(kFull, tbv, src),
-                               rq = __shfl_sync(kFull, rtv, src);
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t ro = __shfl_sync(kFull, row, (int)(j + q < cnt ? j + q : j));
                 x[q] = __ldg(reinterpret_cast<const float4*>(e_item + (size_t)ro * kEmb) + lane);
-                y[q] = __ldg(reinterpret_cast<const float4*>(e_rate + (size_t)rq * kEmb) + lane);
-                z[q] = __ldg(reinterpret_cast<const float4*>(e_date + (size_t)tq * kEmb) + lane);
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < 8; ++q) {
                 if (j + q < cnt) {
-                    acc.x += x[q].x + y[q].x + z[q].x;
-                    acc.y += x[q].y + y[q].y + z[q].y;
-                    acc.z += x[q].z + y[q].z + z[q].z;
-                    acc.w += x[q].w + y[q].w + z[q].w;
+                    acc.x += x[q].x; acc.y += x[q].y; acc.z += x[q].z; acc.w += x[q].w;
                 }
             }
         }
     }
-    const float inv = b > a ? 1.0f / (float)(b - a) : 0.0f;
-    acc.x *= inv; acc.y *= inv; acc.z *= inv; acc.w *= inv;
-    reinterpret_cast<float4*>(h0 + (size_t)w * kEmb)[lane] = acc;
-    __nv_bfloat16* o = h0b + (size_t)w * kEmb + 4 * lane;
-    o[0] = __float2bfloat16(acc.x); o[1] = __float2bfloat16(acc.y);
-    o[2] = __float2bfloat16(acc.z); o[3] = __float2bfloat16(acc.w);
+    part[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        float4 t = part[0][lane];
+#pragma unroll
+        for (int k = 1; k < kBagWarps; ++k) {
+            const float4 v = part[k][lane];
+            t.x += v.x; t.y += v.y; t.z += v.z; t.w += v.w;
+        }
+        for (uint32_t k = 0; k < H; ++k) {
+            const float c = (float)cnt_sh[k];
+            if (c == 0.0f) continue;
+            const float* tab = k < 5 ? e_rate + (size_t)k * kEmb : e_date + (size_t)(k - 5) * kEmb;
+            const float4 v = __ldg(reinterpret_cast<const float4*>(tab) + lane);
+            t.x += c * v.x; t.y += c * v.y; t.z += c * v.z; t.w += c * v.w;
+        }
+        const float inv = b > a ? 1.0f / (float)(b - a) : 0.0f;
+        t.x *= inv; t.y *= inv; t.z *= inv; t.w *= inv;
+        reinterpret_cast<float4*>(h0 + (size_t)w * kEmb)[lane] = t;
+        __nv_bfloat16* o = h0b + (size_t)w * kEmb + 4 * lane;
+        o[0] = __float2bfloat16(t.x); o[1] = __float2bfloat16(t.y);
+        o[2] = __float2bfloat16(t.z); o[3] = __float2bfloat16(t.w);
+        if (lane == 0) inv_n[w] = inv;
+    }
+    for (uint32_t k = threadIdx.x; k < H; k += blockDim.x) hist[(size_t)w * H + k] = (float)cnt_sh[k];
 }
 
-// dE += dh0 / n_u for every rating of every user in the batch: vector atomics
-// into the (item, rating) rows, which users share; the few date-bin rows that
-// every rating hits are summed per block in shared memory first.
-__global__ void __launch_bounds__(256) k_embag_bwd(DeviceState s, const int8_t* __restrict__ raw,
-                                                   const uint32_t* __restrict__ users, int n,
-                                                   const float* __restrict__ dh0, float* __restrict__ g_item,
-                                                   float* __restrict__ g_rate, float* __restrict__ g_date) {
-    __shared__ float sdate[kMaxBins * kEmb];  // T <= kMaxBins date rows
-    const int lane = threadIdx.x & 31;
-    const uint32_t T = s.T;
-    for (uint32_t k = threadIdx.x; k < T * kEmb; k += blockDim.x) sdate[k] = 0.0f;
-    __syncthreads();
-    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const uint32_t u = w < n ? users[w] : 0u;
-    const uint64_t a = w < n ? s.user_off[u] : 0, b = w < n ? s.user_off[u + 1] : 0;
-    if (b > a) {
-        const float inv = 1.0f / (float)(b - a);
-        float4 d = reinterpret_cast<const float4*>(dh0 + (size_t)w * kEmb)[lane];
-        d.x *= inv; d.y *= inv; d.z *= inv; d.w *= inv;
-        float4 rs[5];
-        for (int q = 0; q < 5; ++q) rs[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (uint64_t base = a; base < b; base += 32) {
-            const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
-            uint32_t row = 0, tbv = 0, rtv = 0;
-            if ((uint32_t)lane < cnt) {
-                const Rec r = load_rec(s.rec + base + lane);
-                rtv = (uint32_t)(min(max((int)raw[base + lane], 1), 5) - 1);
-                row = rec_id(r.key) * 5u + rtv;
-                tbv = rec_tbin(r.key);
-            }
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const uint32_t ro = __shfl_sync(kFull, row, (int)j), tb = __shfl_sync(kFull, tbv, (int)j),
-                               rt = __shfl_sync(kFull, rtv, (int)j);
-                float* gi = g_item + (size_t)ro * kEmb + 4 * lane;
-                asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(gi), "f"(d.x), "f"(d.y),
-                             "f"(d.z), "f"(d.w)
-                             : "memory");
-                float* sd = sdate + tb * kEmb + 4 * lane;
-                atomicAdd(sd, d.x); atomicAdd(sd + 1, d.y); atomicAdd(sd + 2, d.z); atomicAdd(sd + 3, d.w);
-#pragma unroll
-                for (int q = 0; q < 5; ++q)
-                    if ((int)rt == q) {
-                        rs[q].x += d.x; rs[q].y += d.y; rs[q].z += d.z; rs[q].w += d.w;
-                    }
-            }
+// dE_item[i, r] += dh0 / n_u for every rating of the user (vector atomics:
+// users share items); one block per user, warps as in the forward pass.
+__global__ void __launch_bounds__(kBagWarps * 32) k_embag_bwd(DeviceState s, const int8_t* __restrict__ raw,
+                                                            const uint32_t* __restrict__ users, int n,
+                                                            const float* __restrict__ dh0,
+                                                            const float* __restrict__ inv_n,
+                                                            float* __restrict__ g_item) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int w = blockIdx.x;
+    const uint32_t u = users[w];
+    const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
+    if (a == b) return;
+    const float inv = inv_n[w];
+    float4 d = reinterpret_cast<const float4*>(dh0 + (size_t)w * kEmb)[lane];
+    d.x *= inv; d.y *= inv; d.z *= inv; d.w *= inv;
+    for (uint64_t base = a + (uint64_t)warp * 32; base < b; base += (uint64_t)kBagWarps * 32) {
+        const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+        uint32_t row = 0;
+        if ((uint32_t)lane < cnt) {
+            const Rec r = load_rec(s.rec + base + lane);
+            row = rec_id(r.key) * 5u + (uint32_t)(min(max((int)raw[base + lane], 1), 5) - 1);
         }
-        for (int q = 0; q < 5; ++q) {
-            float* gr = g_rate + (size_t)q * kEmb + 4 * lane;
-            atomicAdd(gr, rs[q].x); atomicAdd(gr + 1, rs[q].y); atomicAdd(gr + 2, rs[q].z); atomicAdd(gr + 3, rs[q].w);
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const uint32_t ro = __shfl_sync(kFull, row, (int)j);
+            float* gi = g_item + (size_t)ro * kEmb + 4 * lane;
+            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(gi), "f"(d.x), "f"(d.y), "f"(d.z),
+                         "f"(d.w)
+                         : "memory");
         }
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < T * kEmb; k += blockDim.x)
-        if (sdate[k] != 0.0f) atomicAdd(g_date + k, sdate[k]);
+}
+
+// Gradients of the rating and date-bin rows from the histograms:
+// g[k][c] = sum over the batch, in order, of hist[w][k] * dh0[w][c] / n_w
+// (k < 5: rating rows, else date-bin rows). One block per row k.
+__global__ void __launch_bounds__(kEmb) k_hist_grad(const float* __restrict__ hist, uint32_t H,
+                                                    const float* __restrict__ dh0, const float* __restrict__ inv_n,
+                                                    int n, float* __restrict__ g_rate, float* __restrict__ g_date) {
+    const uint32_t k = blockIdx.x, c = threadIdx.x;
+    float acc = 0.0f;
+    int w = 0;
+    for (; w + 4 <= n; w += 4) {
+        float h[4], d[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            h[q] = __ldg(hist + (size_t)(w + q) * H + k) * __ldg(inv_n + w + q);
+            d[q] = __ldg(dh0 + (size_t)(w + q) * kEmb + c);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc += h[q] * d[q];
+    }
+    for (; w < n; ++w) acc += __ldg(hist + (size_t)w * H + k) * __ldg(inv_n + w) * __ldg(dh0 + (size_t)w * kEmb + c);
+    if (k < 5) g_rate[(size_t)k * kEmb + c] = acc;
+    else g_date[(size_t)(k - 5) * kEmb + c] = acc;
 }
 
 // Standardised targets of a batch: [p_u (f), b_u, alpha_u].
@@ -392,6 +416,7 @@ struct tsvd_encoder {
     std::vector<tsvd::Param> params;  // e_item, e_rate, e_date, W1, b1, W2, b2, W3, b3
     tsvd::DevMem raw, mean, inv_std, std_;
     tsvd::DevMem users, h0, h0b, z1, h1b, z2, h2b, y, t, dy, dyb, dh2, dz2b, dh1, dz1b, dh0, part;
+    tsvd::DevMem hist, inv_n;  // per batch user: rating and date-bin counts, 1 / history length
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::string err;
@@ -429,9 +454,10 @@ void forward(tsvd_encoder* e, int n) {
     using namespace tsvd;
     const DeviceState& s = e->model->d;
     cudaStream_t st = e->stream;
-    k_embag_fwd<<<(n + 7) / 8, 256, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n,
-                                             P(e, 0).w.as<float>(), P(e, 1).w.as<float>(), P(e, 2).w.as<float>(),
-                                             e->h0.as<float>(), e->h0b.as<__nv_bfloat16>());
+    k_embag_fwd<<<n, kBagWarps * 32, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n,
+                                              P(e, 0).w.as<float>(), P(e, 1).w.as<float>(), P(e, 2).w.as<float>(),
+                                              e->h0.as<float>(), e->h0b.as<__nv_bfloat16>(), e->hist.as<float>(),
+                                              e->inv_n.as<float>());
     TSVD_CUDA(cudaGetLastError());
     gemm(st, e->h0b.as<__nv_bfloat16>(), 0, kEmb, P(e, 3).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kEmb,
          P(e, 4).w.as<float>(), e->z1.as<float>(), e->h1b.as<__nv_bfloat16>(), kHid, 1);
@@ -477,8 +503,10 @@ double backward(tsvd_encoder* e, int n) {
          e->dh0.as<float>(), nullptr, kEmb, 0);
     // embeddings
     for (int k = 0; k < 3; ++k) TSVD_CUDA(cudaMemsetAsync(P(e, k).g.p, 0, P(e, k).n * 4, st));
-    k_embag_bwd<<<(n + 7) / 8, 256, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n, e->dh0.as<float>(),
-                                             P(e, 0).g.as<float>(), P(e, 1).g.as<float>(), P(e, 2).g.as<float>());
+    k_embag_bwd<<<n, kBagWarps * 32, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n,
+                                              e->dh0.as<float>(), e->inv_n.as<float>(), P(e, 0).g.as<float>());
+    k_hist_grad<<<5 + s.T, kEmb, 0, st>>>(e->hist.as<float>(), 5 + s.T, e->dh0.as<float>(), e->inv_n.as<float>(), n,
+                                          P(e, 1).g.as<float>(), P(e, 2).g.as<float>());
     TSVD_CUDA(cudaGetLastError());
     std::vector<double> part(nb);
     TSVD_CUDA(cudaMemcpyAsync(part.data(), e->part.p, nb * 8, cudaMemcpyDeviceToHost, st));
@@ -619,6 +647,8 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->dz1b.alloc(B * kHid * 2);
         e->dh0.alloc(B * kEmb * 4);
         e->part.alloc(256 * 8);
+        e->hist.alloc((size_t)B * (5 + s.T) * 4);
+        e->inv_n.alloc((size_t)B * 4);
         TSVD_CUDA(cudaDeviceSynchronize());
     });
     if (rc != TSVD_OK) {

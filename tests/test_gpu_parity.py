@@ -117,7 +117,8 @@ def test_gen_preds_offsets(tiny):
     tr, pr = tiny
     cfg = regression_test_config(low_memory=True)
     g = TxModel(tr, MaskedDataset(pr), cfg)
-    pr2 = pr
+    import copy
+    pr2 = copy.copy(pr)  # the session fixture stays untouched
     pr2.residuals = pr.raw_ratings.astype(np.float32) - np.float32(0.25)
     preds = g.gen_preds(pr2)
     base = g.predict_batch(pr.user_idxs, pr.item_idxs, pr.dates)
@@ -137,6 +138,27 @@ def test_stratified_epoch_matches_oracle_tsvdx4p(small, f):
         a = np.asarray(g.get_param(n), np.float64).ravel()
         b = np.asarray(o.get_param(n), np.float64).ravel()
         assert np.max(np.abs(a - b)) < 2e-5, n
+    assert abs(g.calc_rmse(pr) - o.calc_rmse(pr)) < 1e-5
+
+
+@pytest.mark.parametrize("f", [16, 64, 256])
+def test_stratified_heavy_items_match_oracle_tsvdx4p(f):
+    """Items with thousands of ratings take the item stratum's whole-CTA path,
+    whose serial chain runs 32 ratings per round from Gram-matrix lookahead;
+    it must still follow the reference's per-rating item updates."""
+    from tests.conftest import small_sets
+    tr, pr = small_sets(n_users=3000, n_items=80, n_train=90000, seed=13)
+    assert np.bincount(tr.item_idxs, minlength=tr.n_items).max() >= 2048
+    cfg = lm_cfg(f=f, epochs=2)
+    o = po.OracleModel(tr, MaskedDataset(pr), cfg)
+    g = TxModel(tr, MaskedDataset(pr), cfg, schedule=SCHED_STRATIFIED, nsvd_norm_exp=1.0)
+    for e in (1, 2):
+        o.fit_epoch(e, po.SCHED_P, nsvd_norm_exp=1.0, n_threads=1)
+        g.fit_epoch(tr, pr, e)
+    for n in PARAMS + ["ycache", "ycache_bias"]:
+        a = np.asarray(g.get_param(n), np.float64).ravel()
+        b = np.asarray(o.get_param(n), np.float64).ravel()
+        assert np.max(np.abs(a - b) - 1e-5 * np.abs(b)) < 2e-5, n
     assert abs(g.calc_rmse(pr) - o.calc_rmse(pr)) < 1e-5
 
 

@@ -300,6 +300,23 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
 // ---------------------------------------------------------------------------
 constexpr uint32_t kHeavy = 1024;
 constexpr int kRound = 32;  // ratings per buffered round
+constexpr uint32_t kGramStride = kRound + 1;  // padded rows of the per-round Gram matrix
+
+// x = hi + lo with hi, lo in TF32 (round to nearest, ties away from zero).
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    const float rest = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rest));
+}
+
+// d (16x8, FP32) += a (16x8, TF32, row-major) . b (8x8, TF32, column-major)
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
 
 struct ItemState {
     float ib, bt0, bt1, bf0, bf1;
@@ -424,14 +441,17 @@ __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf1
 }
 
 template <int VPL, bool BF>
-__global__ void __launch_bounds__(kThreads) k_item_pass(DeviceState s, EpochParams p, Bf16Copies bf) {
+__global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochParams p, Bf16Copies bf) {
     extern __shared__ float smem[];
     __shared__ uint32_t sh_k;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t Fs = s.Fs, NF = s.NF;
     const uint32_t stride = Fs + 4;       // one staged rating: pe row + {bu_t, cu_t, res, key}
-    float* qfs = smem;                    // [NF][Fs]
-    float* buf = smem + (size_t)NF * Fs;  // [2][kRound][stride]
+    const uint32_t qs = Fs + 4;           // padded q^f row stride (rows of different bins in distinct banks)
+    float* qfs = smem;                    // [NF][qs]
+    float* qsh = qfs + (size_t)NF * qs;   // [Fs] q row of the current round
+    float* buf = qsh + Fs;                // [2][kRound][stride]
+    float* gram = buf + 2ull * kRound * stride;  // [2][kRound][kGramStride]
     for (;;) {
         if (threadIdx.x == 0) sh_k = atomicAdd(&s.counters[2], 1u);
         __syncthreads();
@@ -453,7 +473,7 @@ __global__ void __launch_bounds__(kThreads) k_item_pass(DeviceState s, EpochPara
         }
         // ---------------- heavy item: whole CTA ----------------
         for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
-            qfs[e] = __ldcg(s.ifeat_freq + (size_t)i * NF * Fs + e);
+            qfs[(e / Fs) * qs + e % Fs] = __ldcg(s.ifeat_freq + (size_t)i * NF * Fs + e);
         const uint64_t n = b - a;
         const uint32_t rounds = (uint32_t)((n + kRound - 1) / kRound);
         float q[VPL];
@@ -462,52 +482,226 @@ __global__ void __launch_bounds__(kThreads) k_item_pass(DeviceState s, EpochPara
             Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
             st = load_item_state(s, i, lane);
         }
+        auto round_len = [&](uint32_t r) -> uint32_t {
+            const uint64_t left = n - (uint64_t)r * kRound;
+            return (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
+        };
         auto produce = [&](uint32_t r) {
             float* dst = buf + (size_t)(r & 1) * kRound * stride;
             const uint64_t r0 = a + (uint64_t)r * kRound;
-            const uint64_t left = n - (uint64_t)r * kRound;
-            const uint32_t m = (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
-            for (uint32_t j = warp - 1; j < m; j += kWarps - 1) {
-                const Rec rr = load_rec(s.irec + r0 + j);
-                float pu[VPL], p2[VPL], yc[VPL], pe[VPL];
-                user_rows<VPL, BF>(s, bf, rec_id(rr.key), lane, pu, p2, yc);
-                float bu_t, cu_t;
-                user_scalars(s, rr, bu_t, cu_t);
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) pe[v] = (pu[v] + yc[v]) + rr.dev * p2[v];
+            const uint32_t m = round_len(r);
+            // the round's records and user-side scalars, one rating per lane
+            Rec mine{};
+            float bu_l = 0.0f, cu_l = 0.0f;
+            if ((uint32_t)lane < m) {
+                mine = load_rec(s.irec + r0 + lane);
+                user_scalars(s, mine, bu_l, cu_l);
+            }
+            auto put = [&](uint32_t j, const float (&pu)[VPL], const float (&p2)[VPL], const float (&yc)[VPL]) {
+                const float dev = __shfl_sync(kFull, mine.dev, j), bu = __shfl_sync(kFull, bu_l, j);
+                const float cu = __shfl_sync(kFull, cu_l, j), res = __shfl_sync(kFull, mine.res, j);
+                const uint32_t key = __shfl_sync(kFull, mine.key, j);
                 float* row = dst + (size_t)j * stride;
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) row[Row<VPL>::elem(lane, v)] = pe[v];
+                for (int v = 0; v < VPL; ++v) row[Row<VPL>::elem(lane, v)] = (pu[v] + yc[v]) + dev * p2[v];
                 if (lane == 0) {
-                    row[Fs] = bu_t;
-                    row[Fs + 1] = cu_t;
-                    row[Fs + 2] = rr.res;
-                    row[Fs + 3] = __uint_as_float(rr.key);
+                    row[Fs] = bu;
+                    row[Fs + 1] = cu;
+                    row[Fs + 2] = res;
+                    row[Fs + 3] = __uint_as_float(key);
                 }
+            };
+            // user rows of two ratings in flight per warp
+            for (uint32_t j0 = warp - 1; j0 < m; j0 += 2 * (kWarps - 1)) {
+                const uint32_t j1 = j0 + (kWarps - 1);
+                const bool two = j1 < m;
+                const uint32_t u0 = rec_id(__shfl_sync(kFull, mine.key, j0));
+                const uint32_t u1 = rec_id(__shfl_sync(kFull, mine.key, two ? j1 : j0));
+                float pa[VPL], p2a[VPL], yca[VPL], pb[VPL], p2b[VPL], ycb[VPL];
+                user_rows<VPL, BF>(s, bf, u0, lane, pa, p2a, yca);
+                if (two) user_rows<VPL, BF>(s, bf, u1, lane, pb, p2b, ycb);
+                put(j0, pa, p2a, yca);
+                if (two) put(j1, pb, p2b, ycb);
+            }
+            // rows m..31 of a partial round are zero (finite values for the
+            // consumer's unconditional loops)
+            for (uint32_t j = m + warp - 1; j < (uint32_t)kRound; j += kWarps - 1) {
+                float* row = dst + (size_t)j * stride;
+                for (uint32_t e = lane; e < stride; e += 32) row[e] = 0.0f;
+            }
+            // all rows of the round are in place before the Gram products
+            asm volatile("bar.sync 1, %0;" ::"r"((kWarps - 1) * 32) : "memory");
+            // G = PE PE^T for the round's ratings, on the tensor cores: TF32
+            // operands split into high and low parts, three products per
+            // tile (error near FP32's). Producer warp w takes tile w - 1 of
+            // the six 16x8 tiles that hold the pairs k < j.
+            const int tile = warp - 1;
+            if (tile < 6) {
+                float* gm = gram + (size_t)(r & 1) * kRound * kGramStride;
+                const int mt = tile < 4 ? 0 : 1, nt = tile < 4 ? tile : tile - 2;
+                const int gid = lane >> 2, tig = lane & 3;
+                const float* A0 = dst + (size_t)(mt * 16 + gid) * stride;
+                const float* A1 = A0 + 8 * (size_t)stride;
+                const float* B0 = dst + (size_t)(nt * 8 + gid) * stride;
+                float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 4
+                for (uint32_t k0 = 0; k0 < Fs; k0 += 8) {
+                    uint32_t ah[4], al[4], bh[2], bl[2];
+                    split_tf32(A0[k0 + tig], ah[0], al[0]);
+                    split_tf32(A1[k0 + tig], ah[1], al[1]);
+                    split_tf32(A0[k0 + tig + 4], ah[2], al[2]);
+                    split_tf32(A1[k0 + tig + 4], ah[3], al[3]);
+                    split_tf32(B0[k0 + tig], bh[0], bl[0]);
+                    split_tf32(B0[k0 + tig + 4], bh[1], bl[1]);
+                    mma_tf32(d, al, bh);
+                    mma_tf32(d, ah, bl);
+                    mma_tf32(d, ah, bh);
+                }
+                float* g0 = gm + (size_t)(mt * 16 + gid) * kGramStride + nt * 8 + 2 * tig;
+                g0[0] = d[0];
+                g0[1] = d[1];
+                g0[8 * kGramStride] = d[2];
+                g0[8 * kGramStride + 1] = d[3];
             }
         };
         if (warp > 0) produce(0);
         __syncthreads();
         const float gb = s.gbias;
+        // update factors: x - lr (g + reg x) = a x - lr g
+        const float a_i = 1.0f - p.lr_i * p.reg_i, a_f = 1.0f - p.lr_iqf * p.reg_iqf;
         for (uint32_t r = 0; r < rounds; ++r) {
             if (warp > 0) {
                 if (r + 1 < rounds) produce(r + 1);
             } else {
+                // Lookahead over the round's m ratings (all of one item): with
+                // q_k, qf_k the item rows before rating k, and pe_k fixed in
+                // the item stratum,
+                //   q_k . pe_k = a_i^k (q_0 . pe_k) - lr_i sum_{j<k} a_i^(k-1-j) err_j G_jk
+                // and likewise for the q^f row of pe_k's frequency bin over the
+                // earlier ratings of the same bin. The dots with q_0 are taken
+                // once per round; the serial chain is then scalar per rating,
+                // and the round's updates are applied in closed form,
+                //   q_m = a_i^m q_0 - lr_i sum_k a_i^(m-1-k) err_k pe_k.
+                // Rows m..31 of a partial round are zero.
                 const float* src = buf + (size_t)(r & 1) * kRound * stride;
-                const uint64_t left = n - (uint64_t)r * kRound;
-                const uint32_t m = (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
-                for (uint32_t j = 0; j < m; ++j) {
-                    const float* row = src + (size_t)j * stride;
-                    float pe[VPL];
+                const float* gm = gram + (size_t)(r & 1) * kRound * kGramStride;
+                const uint32_t m = round_len(r);
+                const float* myrow = src + (size_t)lane * stride;
+                const float bu_t = myrow[Fs], cu_t = myrow[Fs + 1], res = myrow[Fs + 2];
+                const uint32_t key = __float_as_uint(myrow[Fs + 3]);
+                const uint32_t tb = rec_tbin(key), fb = rec_fbin(key);
+                // this lane's dots with q_0 and q^f_0[fb]: the round's q row
+                // goes to shared memory, and each lane walks its own pe row
 #pragma unroll
-                    for (int v = 0; v < VPL; ++v) pe[v] = row[Row<VPL>::elem(lane, v)];
-                    const float bu_t = row[Fs], cu_t = row[Fs + 1], res = row[Fs + 2];
-                    const uint32_t key = __float_as_uint(row[Fs + 3]);
-                    const uint32_t tb = rec_tbin(key), fb = rec_fbin(key);
-                    float* qrow = qfs + (size_t)fb * Fs;
-                    item_step<VPL>(p, gb, q, [&](int v) -> float& { return qrow[Row<VPL>::elem(lane, v)]; }, pe,
-                                   bu_t, cu_t, res, tb, fb, lane, st);
+                for (int v = 0; v < VPL; ++v) qsh[Row<VPL>::elem(lane, v)] = q[v];
+                __syncwarp();
+                float sq, sf;
+                {
+                    const float4* x4 = reinterpret_cast<const float4*>(myrow);
+                    const float4* y4 = reinterpret_cast<const float4*>(qsh);
+                    const float4* z4 = reinterpret_cast<const float4*>(qfs + (size_t)fb * qs);
+                    float s0 = 0.0f, s1 = 0.0f, e0 = 0.0f, e1 = 0.0f;
+#pragma unroll 4
+                    for (uint32_t k4 = 0; k4 < Fs / 4; ++k4) {
+                        const float4 x = x4[k4], y = y4[k4], z = z4[k4];
+                        s0 = fmaf(x.x, y.x, s0);
+                        s1 = fmaf(x.y, y.y, s1);
+                        s0 = fmaf(x.z, y.z, s0);
+                        s1 = fmaf(x.w, y.w, s1);
+                        e0 = fmaf(x.x, z.x, e0);
+                        e1 = fmaf(x.y, z.y, e1);
+                        e0 = fmaf(x.z, z.z, e0);
+                        e1 = fmaf(x.w, z.w, e1);
+                    }
+                    sq = s0 + s1;  // q_0 . pe_lane
+                    sf = e0 + e1;  // qf_0[fb] . pe_lane
                 }
+                float c = 0.0f, cf = 0.0f;
+                float ib = st.ib;
+                float bit = __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31);
+                float ibf = __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
+                float my_err = 0.0f, my_ec = 0.0f;
+                float pw = 1.0f, pwf = 1.0f, am = 1.0f;  // a_i^(m-1-lane), a_f^(later same-bin), a_i^m
+                for (uint32_t k = 0; k < m; ++k) {
+                    const float g = gm[k * kGramStride + lane];
+                    const uint32_t tbk = __shfl_sync(kFull, tb, k), fbk = __shfl_sync(kFull, fb, k);
+                    const float dot = (sq - p.lr_i * c) + (sf - p.lr_iqf * cf);
+                    const float err = (gb + bu_t + (ib + bit + ibf) * cu_t + dot) - res;
+                    const float ec = err * cu_t;
+                    if (lane == (int)k) {
+                        my_err = err;
+                        my_ec = ec;
+                    }
+                    const float ek = __shfl_sync(kFull, err, k), eck = __shfl_sync(kFull, ec, k);
+                    sq *= a_i;
+                    c = fmaf(a_i, c, ek * g);
+                    am *= a_i;
+                    if (k > (uint32_t)lane) pw *= a_i;
+                    if (fb == fbk) {
+                        sf *= a_f;
+                        cf = fmaf(a_f, cf, ek * g);
+                        ibf -= p.lr_ibf * eck;
+                        if (k > (uint32_t)lane) pwf *= a_f;
+                    }
+                    if (tb == tbk) bit -= p.lr_ti * eck;
+                    ib -= p.lr_ib * eck;
+                }
+                const bool valid = lane < (int)m;
+                const float wq = valid ? p.lr_i * pw * my_err : 0.0f;
+                const float wf = valid ? p.lr_iqf * pwf * my_err : 0.0f;
+                const float wb = valid ? my_ec : 0.0f;
+                // biases
+                st.ib -= p.lr_ib * warp_sum(wb);
+                {
+                    float dt0 = 0.0f, dt1 = 0.0f, df0 = 0.0f, df1 = 0.0f;
+#pragma unroll 4
+                    for (int k = 0; k < kRound; ++k) {
+                        const float e = __shfl_sync(kFull, wb, k);
+                        const uint32_t tbk = __shfl_sync(kFull, tb, k), fbk = __shfl_sync(kFull, fb, k);
+                        if (lane == (int)(tbk & 31)) {
+                            if (tbk < 32) dt0 += e;
+                            else dt1 += e;
+                        }
+                        if (lane == (int)(fbk & 31)) {
+                            if (fbk < 32) df0 += e;
+                            else df1 += e;
+                        }
+                    }
+                    st.bt0 -= p.lr_ti * dt0;
+                    st.bt1 -= p.lr_ti * dt1;
+                    st.bf0 -= p.lr_ibf * df0;
+                    st.bf1 -= p.lr_ibf * df1;
+                }
+                // q
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) q[v] *= am;
+#pragma unroll 4
+                for (int k = 0; k < kRound; ++k) {
+                    const float w = __shfl_sync(kFull, wq, k);
+                    float pk[VPL];
+                    row_from_smem<VPL>(src + (size_t)k * stride, lane, pk);
+#pragma unroll
+                    for (int v = 0; v < VPL; ++v) q[v] = fmaf(-w, pk[v], q[v]);
+                }
+                // q^f rows: the first rating of a bin also applies the bin's decay
+                const unsigned same = __match_any_sync(kFull, valid ? fb : 64u + (uint32_t)lane);
+                float dec = 1.0f;
+                if (valid && __ffs(same) - 1 == lane)
+                    for (int z = __popc(same); z > 0; --z) dec *= a_f;
+#pragma unroll 2
+                for (int k = 0; k < kRound; ++k) {
+                    const float w = __shfl_sync(kFull, wf, k), dk = __shfl_sync(kFull, dec, k);
+                    const uint32_t f = __shfl_sync(kFull, fb, k);
+                    float* qrow = qfs + (size_t)f * qs;
+                    float row[VPL], pk[VPL];
+                    row_from_smem<VPL>(qrow, lane, row);
+                    row_from_smem<VPL>(src + (size_t)k * stride, lane, pk);
+#pragma unroll
+                    for (int v = 0; v < VPL; ++v) row[v] = fmaf(-w, pk[v], dk * row[v]);
+#pragma unroll
+                    for (int v = 0; v < VPL; ++v) qrow[Row<VPL>::elem(lane, v)] = row[v];
+                }
+                __syncwarp();
             }
             __syncthreads();
         }
@@ -516,7 +710,7 @@ __global__ void __launch_bounds__(kThreads) k_item_pass(DeviceState s, EpochPara
             store_item_state(s, i, lane, st);
         }
         for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
-            __stcg(s.ifeat_freq + (size_t)i * NF * Fs + e, qfs[e]);
+            __stcg(s.ifeat_freq + (size_t)i * NF * Fs + e, qfs[(e / Fs) * qs + e % Fs]);
         __syncthreads();
     }
 }
@@ -557,7 +751,9 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     }
     {
         ProfScope ps(m, "item_pass");
-        const size_t smem = ((size_t)s.NF * s.Fs + 2ull * kRound * (s.Fs + 4)) * sizeof(float);
+        const size_t smem =
+            ((size_t)s.NF * (s.Fs + 4) + s.Fs + 2ull * kRound * (s.Fs + 4) + 2ull * kRound * kGramStride) *
+            sizeof(float);
         TSVD_CUDA(cudaFuncSetAttribute(k_item_pass<VPL, BFU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         unsigned g = persistent_grid(k_item_pass<VPL, BFU>, smem);
         k_item_pass<VPL, BFU><<<g, kThreads, smem, m->stream>>>(s, p, bf);

@@ -543,25 +543,33 @@ __global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochP
                 const float* A0 = dst + (size_t)(mt * 16 + gid) * stride;
                 const float* A1 = A0 + 8 * (size_t)stride;
                 const float* B0 = dst + (size_t)(nt * 8 + gid) * stride;
-                float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll 4
-                for (uint32_t k0 = 0; k0 < Fs; k0 += 8) {
-                    uint32_t ah[4], al[4], bh[2], bl[2];
-                    split_tf32(A0[k0 + tig], ah[0], al[0]);
-                    split_tf32(A1[k0 + tig], ah[1], al[1]);
-                    split_tf32(A0[k0 + tig + 4], ah[2], al[2]);
-                    split_tf32(A1[k0 + tig + 4], ah[3], al[3]);
-                    split_tf32(B0[k0 + tig], bh[0], bl[0]);
-                    split_tf32(B0[k0 + tig + 4], bh[1], bl[1]);
-                    mma_tf32(d, al, bh);
-                    mma_tf32(d, ah, bl);
-                    mma_tf32(d, ah, bh);
+                // independent accumulators: the three split products and
+                // even/odd k-steps run as separate MMA chains
+                float d[6][4] = {};
+#pragma unroll 2
+                for (uint32_t k0 = 0; k0 < Fs; k0 += 16) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t kk = k0 + 8 * h;
+                        uint32_t ah[4], al[4], bh[2], bl[2];
+                        split_tf32(A0[kk + tig], ah[0], al[0]);
+                        split_tf32(A1[kk + tig], ah[1], al[1]);
+                        split_tf32(A0[kk + tig + 4], ah[2], al[2]);
+                        split_tf32(A1[kk + tig + 4], ah[3], al[3]);
+                        split_tf32(B0[kk + tig], bh[0], bl[0]);
+                        split_tf32(B0[kk + tig + 4], bh[1], bl[1]);
+                        mma_tf32(d[3 * h], al, bh);
+                        mma_tf32(d[3 * h + 1], ah, bl);
+                        mma_tf32(d[3 * h + 2], ah, bh);
+                    }
                 }
+#pragma unroll
+                for (int e = 0; e < 4; ++e) d[0][e] = ((d[0][e] + d[1][e]) + (d[3][e] + d[4][e])) + (d[2][e] + d[5][e]);
                 float* g0 = gm + (size_t)(mt * 16 + gid) * kGramStride + nt * 8 + 2 * tig;
-                g0[0] = d[0];
-                g0[1] = d[1];
-                g0[8 * kGramStride] = d[2];
-                g0[8 * kGramStride + 1] = d[3];
+                g0[0] = d[0][0];
+                g0[1] = d[0][1];
+                g0[8 * kGramStride] = d[0][2];
+                g0[8 * kGramStride + 1] = d[0][3];
             }
         };
         if (warp > 0) produce(0);
@@ -616,37 +624,46 @@ __global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochP
                     sq = s0 + s1;  // q_0 . pe_lane
                     sf = e0 + e1;  // qf_0[fb] . pe_lane
                 }
-                float c = 0.0f, cf = 0.0f;
-                float ib = st.ib;
-                float bit = __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31);
-                float ibf = __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
-                float my_err = 0.0f, my_ec = 0.0f;
-                float pw = 1.0f, pwf = 1.0f, am = 1.0f;  // a_i^(m-1-lane), a_f^(later same-bin), a_i^m
-                for (uint32_t k = 0; k < m; ++k) {
-                    const float g = gm[k * kGramStride + lane];
-                    const uint32_t tbk = __shfl_sync(kFull, tb, k), fbk = __shfl_sync(kFull, fb, k);
-                    const float dot = (sq - p.lr_i * c) + (sf - p.lr_iqf * cf);
-                    const float err = (gb + bu_t + (ib + bit + ibf) * cu_t + dot) - res;
-                    const float ec = err * cu_t;
-                    if (lane == (int)k) {
-                        my_err = err;
-                        my_ec = ec;
-                    }
-                    const float ek = __shfl_sync(kFull, err, k), eck = __shfl_sync(kFull, ec, k);
-                    sq *= a_i;
-                    c = fmaf(a_i, c, ek * g);
-                    am *= a_i;
-                    if (k > (uint32_t)lane) pw *= a_i;
-                    if (fb == fbk) {
-                        sf *= a_f;
-                        cf = fmaf(a_f, cf, ek * g);
-                        ibf -= p.lr_ibf * eck;
-                        if (k > (uint32_t)lane) pwf *= a_f;
-                    }
-                    if (tb == tbk) bit -= p.lr_ti * eck;
-                    ib -= p.lr_ib * eck;
-                }
+                // The round's errors solve a unit lower-triangular system
+                // err = C - M err: C_j holds everything known at the round's
+                // start, M_ji (i < j) the effect of err_i on rating j through
+                // q, q^f of the same bin and the item biases. Forward
+                // substitution then costs one broadcast and one FMA per rating.
                 const bool valid = lane < (int)m;
+                float Mrow[kRound];
+                float pw_d = 1.0f, pwf_d = 1.0f;  // a_i^(j-1-i), a_f^(same-bin ratings between i and j)
+#pragma unroll
+                for (int i = kRound - 1; i >= 0; --i) {
+                    const float gij = gm[i * kGramStride + lane];
+                    const float cui = __shfl_sync(kFull, cu_t, i);
+                    const uint32_t ti = __shfl_sync(kFull, tb, i), fi = __shfl_sync(kFull, fb, i);
+                    const bool before = i < lane, same_f = fi == fb, same_t = ti == tb;
+                    const float bias_lr = p.lr_ib + (same_t ? p.lr_ti : 0.0f) + (same_f ? p.lr_ibf : 0.0f);
+                    const float v = cu_t * cui * bias_lr + p.lr_i * pw_d * gij + (same_f ? p.lr_iqf * pwf_d * gij : 0.0f);
+                    Mrow[i] = before ? v : 0.0f;
+                    if (before) {
+                        pw_d *= a_i;
+                        if (same_f) pwf_d *= a_f;
+                    }
+                }
+                // pw_d = a_i^j, pwf_d = a_f^(earlier ratings of the same bin)
+                const float bi0 = st.ib + __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31) +
+                                  __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
+                float x = ((gb + bu_t + bi0 * cu_t) + (pw_d * sq + pwf_d * sf)) - res;
+                x = valid ? x : 0.0f;
+#pragma unroll
+                for (int i = 0; i < kRound; ++i) x = fmaf(-Mrow[i], __shfl_sync(kFull, x, i), x);
+                const float my_err = x, my_ec = x * cu_t;
+                // weights of the closed-form updates: a_i^(m-1-j), a_f^(later ratings of the same bin), a_i^m
+                float pw = 1.0f, pwf = 1.0f, am = 1.0f;
+#pragma unroll
+                for (int i = 0; i < kRound; ++i) {
+                    const uint32_t fi = __shfl_sync(kFull, fb, i);
+                    const bool inr = i < (int)m, after = inr && i > lane;
+                    am = inr ? am * a_i : am;
+                    pw = after ? pw * a_i : pw;
+                    pwf = (after && fi == fb) ? pwf * a_f : pwf;
+                }
                 const float wq = valid ? p.lr_i * pw * my_err : 0.0f;
                 const float wf = valid ? p.lr_iqf * pwf * my_err : 0.0f;
                 const float wb = valid ? my_ec : 0.0f;
@@ -658,14 +675,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochP
                     for (int k = 0; k < kRound; ++k) {
                         const float e = __shfl_sync(kFull, wb, k);
                         const uint32_t tbk = __shfl_sync(kFull, tb, k), fbk = __shfl_sync(kFull, fb, k);
-                        if (lane == (int)(tbk & 31)) {
-                            if (tbk < 32) dt0 += e;
-                            else dt1 += e;
-                        }
-                        if (lane == (int)(fbk & 31)) {
-                            if (fbk < 32) df0 += e;
-                            else df1 += e;
-                        }
+                        dt0 += lane == (int)tbk ? e : 0.0f;
+                        dt1 += lane + 32 == (int)tbk ? e : 0.0f;
+                        df0 += lane == (int)fbk ? e : 0.0f;
+                        df1 += lane + 32 == (int)fbk ? e : 0.0f;
                     }
                     st.bt0 -= p.lr_ti * dt0;
                     st.bt1 -= p.lr_ti * dt1;

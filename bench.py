@@ -232,6 +232,36 @@ def cpu_baseline(args):
                       f"{args.shape} generator, f={args.f}; host has {os.cpu_count()} cores"}
 
 
+def l2_read_gbs(stream) -> float:
+    """Streaming read bandwidth of an L2-resident buffer (48 MB of FP32, summed
+    50 times by torch on the bench's stream): the on-chip counterpart of the
+    HBM copy peak, for kernels whose working set L2 serves."""
+    import torch
+    x = torch.empty(12 * 1024 * 1024, dtype=torch.float32, device="cuda").uniform_()
+    with torch.cuda.stream(stream):
+        for _ in range(5):
+            x.sum()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(50):
+            x.sum()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return 50 * x.numel() * 4 / (e0.elapsed_time(e1) / 1000.0) / 1e9
+
+
+def user_pass_l2(kstats, args, R, l2):
+    """The per-user passes against the L2 figure: item-side bytes per rating
+    (Hogwild: q, q^f read + write and y gather + RMW, 28 f; stratified user
+    stratum: q, q^f reads, 8 f) over the pass's duration."""
+    out = {}
+    for kn, bpr in (("user_pass_hogwild", 28 * args.f), ("user_pass_stratified", 8 * args.f)):
+        if kn in kstats:
+            gbs = bpr * R / (kstats[kn]["avg_ms"] / 1000.0) / 1e9
+            out[kn] = {"item_side_bytes_per_rating": bpr, "achieved_gbs": gbs, "frac_of_l2_read": gbs / l2}
+    return out
+
+
 def time_to_rmse(model, tr, pr):
     """Time to a held-out RMSE target for new users (the C5 fold-in): the
     plain form (standard init + user-side SGD passes with item tables frozen)
@@ -317,17 +347,13 @@ def main():
     R = tr.n_ratings
     cfg = run_lm(args.f, args.warmup + args.steps, n_time_bins=30)
 
+    from netflix_prize_b200 import dist
+
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
+        dist.barrier(world)
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return dist.max_over_ranks(x, world)
 
     stream = torch.cuda.current_stream()
     # ---------------- value: device-resident epochs ----------------
@@ -360,6 +386,7 @@ def main():
     rmse = model.calc_rmse(pr)
     value = R * args.steps * world / (ms / 1000.0)
     peak, peak_kind = measured_peaks()
+    l2 = l2_read_gbs(stream)
     dom = kstats.get(kname, {"avg_ms": float("nan")})
     bpr = kernel_bytes_per_rating(kname, args.f)
     achieved = bpr * R / (dom["avg_ms"] / 1000.0) / 1e9
@@ -415,7 +442,9 @@ def main():
         "config": workload_config(args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": kname,
-                     "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_rating": bpr},
+                     "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_rating": bpr,
+                     "l2_read_gbs": l2, "l2_source": "bench: torch sum over a 48 MB L2-resident buffer",
+                     "user_pass_vs_l2": user_pass_l2(kstats, args, R, l2)},
         "kernels": kstats,
         "heldout_rmse_after_run": rmse,
         "clocks": clk,

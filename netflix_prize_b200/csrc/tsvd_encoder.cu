@@ -15,9 +15,10 @@
 //
 // Loss: mean squared error against the standardised targets. Weights are FP32
 // masters with BF16 copies; every GEMM runs on the tensor cores with BF16
-// operands and FP32 accumulation (mma.sync m16n8k16), activations are stored
-// as BF16 for the next GEMM and as FP32 pre-activations for the GELU
-// derivative. AdamW updates all parameters (weight decay on the matrices).
+// operands and an FP32 accumulator in tensor memory (tcgen05.mma, 128x128
+// tiles), activations are stored as BF16 for the next GEMM and as FP32
+// pre-activations for the GELU derivative. AdamW updates all parameters
+// (weight decay on the matrices).
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -39,14 +40,10 @@ constexpr int kEmb = 128, kHid = 512, kMaxBatch = 4096;
 // ---------------------------------------------------------------------------
 // C[M,N] = op(A)[M,K] . op(B)[K,N] with BF16 operands, FP32 accumulation.
 // A is [M,K] row-major (a_km = 0) or stored as [K,M] (a_km = 1); B is stored
-// as [K,N] (b_kn = 1) or [N,K] (b_kn = 0). 64x64 tiles, BK = 32, 4 warps of
-// 32x32, operands staged in shared memory as [64][BK] rows (B transposed) and
-// fed to mma.sync through ldmatrix.
+// as [K,N] (b_kn = 1) or [N,K] (b_kn = 0).
 // Epilogue: + bias[n] (optional); out_f32 and/or out_bf16 (optional); with
 // gelu, out_f32 receives the pre-activation and out_bf16 GELU of it.
 // ---------------------------------------------------------------------------
-constexpr int TM = 64, TN = 64, TK = 32, TKP = TK + 8;
-
 struct GemmArgs {
     const __nv_bfloat16* A;
     const __nv_bfloat16* B;
@@ -64,100 +61,219 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return cdf + x * pdf;
 }
 
-__device__ __forceinline__ void ldmatrix_x4(unsigned (&r)[4], const void* p) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-__device__ __forceinline__ void ldmatrix_x2(unsigned (&r)[2], const void* p) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
-}
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+// ---------------------------------------------------------------------------
+// The GEMM runs on the 5th-generation tensor cores (tcgen05): a 128x64 output
+// tile per CTA with its FP32 accumulator in tensor memory. Each 64-deep K block
+// of A and B is staged in shared memory as BF16 in the K-major, unswizzled
+// core-matrix layout (a core matrix is 8 rows x 16 bytes; core matrices are
+// 128 B apart along K and 1024 B apart along M or N). Two stages: while one
+// thread's four tcgen05.mma (M = 128, N = 64, K = 16) run on one stage, all
+// threads fill the other; each stage's MMAs are committed to its own mbarrier,
+// which is waited on (with an iteration limit) before the stage is refilled.
+// The epilogue reads the accumulator back with tcgen05.ld, one row per thread.
+// ---------------------------------------------------------------------------
+constexpr int TC_M = 128, TC_N = 64, TC_K = 64;
+constexpr uint32_t kTcABytes = TC_M * TC_K * 2;        // 16 KB A tile per stage
+constexpr uint32_t kTcBBytes = TC_N * TC_K * 2;        // 8 KB B tile per stage
+constexpr uint32_t kTcStage = kTcABytes + kTcBBytes;
+constexpr uint32_t kTcLBO = 128;                       // core matrices adjacent along K
+constexpr uint32_t kTcSBO = (TC_K / 8) * 128;          // core matrices adjacent along M / N
+constexpr uint32_t kTcSmem = 56 * 1024;                // 2 stages + mbarriers + TMEM address; caps residency
+                                                       // at 4 CTAs per SM, whose 4 x 64 TMEM columns always fit
+constexpr unsigned kTcWaitLimit = 1u << 20;
+// instruction descriptor: D FP32, A and B BF16, both K-major, N = 64, M = 128
+constexpr uint32_t kTcIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of element (row r, k) of a staged tile
+__device__ __forceinline__ uint32_t tc_off(int r, int k) {
+    return (uint32_t)(r >> 3) * kTcSBO + (uint32_t)(k >> 3) * kTcLBO + (uint32_t)(r & 7) * 16u + (uint32_t)(k & 7) * 2u;
 }
 
-__global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
-    __shared__ __align__(16) __nv_bfloat16 As[TM][TKP];
-    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TKP];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    float acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-    for (int k0 = 0; k0 < g.K; k0 += TK) {
-        for (int e = tid; e < TM * TK; e += 128) {
-            const int r = e / TK, c = e % TK;
-            const int gm = m0 + r, gk = k0 + c;
-            __nv_bfloat16 v = zero;
-            if (gm < g.M && gk < g.K) v = g.a_km ? g.A[(size_t)gk * g.lda + gm] : g.A[(size_t)gm * g.lda + gk];
-            As[r][c] = v;
-        }
-        for (int e = tid; e < TN * TK; e += 128) {
-            const int r = e / TK, c = e % TK;
-            const int gn = n0 + r, gk = k0 + c;
-            __nv_bfloat16 v = zero;
-            if (gn < g.N && gk < g.K) v = g.b_kn ? g.B[(size_t)gk * g.ldb + gn] : g.B[(size_t)gn * g.ldb + gk];
-            Bs[r][c] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < TK; kk += 16) {
-            unsigned af[2][4], bfr[4][2];
-#pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const int row = wm + a * 16 + (lane & 15);
-                const int col = kk + ((lane >> 4) << 3);
-                ldmatrix_x4(af[a], &As[row][col]);
-            }
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int row = wn + b * 8 + (lane & 7);
-                const int col = kk + (((lane >> 3) & 1) << 3);
-                ldmatrix_x2(bfr[b], &Bs[row][col]);
-            }
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) mma_bf16(acc[a][b], af[a], bfr[b]);
-        }
-        __syncthreads();
+// shared-memory matrix descriptor: start address, leading (K) and stride (M/N)
+// byte offsets in 16-byte units, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((kTcLBO >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((kTcSBO >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase) {
+    for (unsigned it = 0; it < kTcWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{.reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p;}"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
     }
-    // accumulator layout of m16n8: c0,c1 -> row lane/4, cols 2*(lane%4)+{0,1}; c2,c3 -> row lane/4 + 8
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const int m = m0 + wm + a * 16 + (lane >> 2) + h * 8;
-                    const int n = n0 + wn + b * 8 + 2 * (lane & 3) + c;
-                    if (m >= g.M || n >= g.N) continue;
-                    float v = acc[a][b][h * 2 + c];
-                    if (g.bias) v += g.bias[n];
-                    if (g.out_f32) g.out_f32[(size_t)m * g.ldc + n] = v;
-                    if (g.out_bf16) g.out_bf16[(size_t)m * g.ldc + n] = __float2bfloat16(g.gelu ? gelu_f(v) : v);
-                }
+    return false;
 }
 
-void gemm(cudaStream_t st, const __nv_bfloat16* A, int a_km, int lda, const __nv_bfloat16* B, int b_kn, int ldb, int M,
+// Fill a (ROWS x TC_K) tile with rows r0.. and k0.. of X (zero outside), X
+// stored [rows][K] (x_km = 0) or [K][rows] (x_km = 1); 16-byte loads along
+// X's contiguous dimension where the layout allows.
+template <int ROWS>
+__device__ __forceinline__ void tc_stage(const __nv_bfloat16* X, int x_km, int ld, int rows, int K, int r0, int k0,
+                                         uint8_t* tile, int tid) {
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    const bool vec = (ld & 7) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+    if (vec && !x_km) {
+        // 8 consecutive k of one row = one core-matrix row (16 bytes)
+        for (int e = tid; e < ROWS * (TC_K / 8); e += 128) {
+            const int r = e / (TC_K / 8), k8 = (e % (TC_K / 8)) * 8;
+            const int gr = r0 + r, gk = k0 + k8;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (gr < rows) {
+                if (gk + 8 <= K) {
+                    v = __ldg(reinterpret_cast<const uint4*>(X + (size_t)gr * ld + gk));
+                } else {
+                    __nv_bfloat16 t[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) t[q] = gk + q < K ? X[(size_t)gr * ld + gk + q] : zero;
+                    v = *reinterpret_cast<const uint4*>(t);
+                }
+            }
+            *reinterpret_cast<uint4*>(tile + tc_off(r, k8)) = v;
+        }
+    } else if (vec) {
+        // 8 consecutive rows at one k: one column of a core matrix
+        for (int e = tid; e < (ROWS / 8) * TC_K; e += 128) {
+            const int r8 = (e % (ROWS / 8)) * 8, k = e / (ROWS / 8);
+            const int gr = r0 + r8, gk = k0 + k;
+            __nv_bfloat16 t[8];
+            if (gk < K && gr + 8 <= rows) {
+                *reinterpret_cast<uint4*>(t) = __ldg(reinterpret_cast<const uint4*>(X + (size_t)gk * ld + gr));
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) t[q] = (gk < K && gr + q < rows) ? X[(size_t)gk * ld + gr + q] : zero;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(r8 + q, k)) = t[q];
+        }
+    } else {
+        for (int e = tid; e < ROWS * TC_K; e += 128) {
+            // consecutive threads take consecutive rows when X is stored [K][rows]
+            const int r = x_km ? e % ROWS : e / TC_K, k = x_km ? e / ROWS : e % TC_K;
+            const int gr = r0 + r, gk = k0 + k;
+            __nv_bfloat16 v = zero;
+            if (gr < rows && gk < K) v = x_km ? X[(size_t)gk * ld + gr] : X[(size_t)gr * ld + gk];
+            *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(r, k)) = v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) uint8_t tsm[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 2 * kTcStage);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tsm + 2 * kTcStage + 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * TC_N;
+    const uint32_t s_base = smem_u32(tsm), mb0 = smem_u32(mbar), mb1 = mb0 + 8;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)TC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    const int nk = (g.K + TC_K - 1) / TC_K;
+    tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, 0, tsm, tid);
+    tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, 0, tsm + kTcABytes, tid);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    for (int kb = 0; kb < nk && ok; ++kb) {
+        const uint32_t st = (uint32_t)(kb & 1);
+        if (tid == 0) {
+            const uint32_t a_s = s_base + st * kTcStage, b_s = a_s + kTcABytes;
+#pragma unroll
+            for (int kk = 0; kk < TC_K / 16; ++kk) {
+                const uint64_t ad = tc_desc(a_s + (uint32_t)kk * 2u * kTcLBO);
+                const uint64_t bd = tc_desc(b_s + (uint32_t)kk * 2u * kTcLBO);
+                const uint32_t accumulate = (kb > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{.reg .pred p; setp.ne.u32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;}" ::"r"(
+                        tmem),
+                    "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(accumulate));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             st ? mb1 : mb0)
+                         : "memory");
+        }
+        if (kb + 1 < nk) {
+            // the other stage was read by block kb - 1's MMAs
+            if (kb >= 1) {
+                const uint32_t ps = (uint32_t)((kb - 1) & 1), par = (uint32_t)(((kb - 1) >> 1) & 1);
+                ok = __syncthreads_and(tc_wait(ps ? mb1 : mb0, par) ? 1 : 0) != 0;
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;");
+            }
+            uint8_t* nxt = tsm + (st ^ 1u) * kTcStage;
+            tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, (kb + 1) * TC_K, nxt, tid);
+            tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, (kb + 1) * TC_K, nxt + kTcABytes, tid);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;");
+        }
+    }
+    if (ok) {
+        // the last commit covers every MMA issued before it
+        const uint32_t ls = (uint32_t)((nk - 1) & 1), par = (uint32_t)(((nk - 1) >> 1) & 1);
+        ok = __syncthreads_and(tc_wait(ls ? mb1 : mb0, par) ? 1 : 0) != 0;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(err, 1u);
+        const uint32_t ls = (uint32_t)((nk - 1) & 1), par = (uint32_t)(((nk - 1) >> 1) & 1);
+        tc_wait(ls ? mb1 : mb0, par);  // one more bounded wait for the MMAs in flight
+    } else {
+        const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_N; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < g.M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= g.N) continue;
+                    float x = __uint_as_float(v[j]);
+                    if (g.bias) x += g.bias[n];
+                    if (g.out_f32) g.out_f32[(size_t)m * g.ldc + n] = x;
+                    if (g.out_bf16) g.out_bf16[(size_t)m * g.ldc + n] = __float2bfloat16(g.gelu ? gelu_f(x) : x);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TC_N));
+}
+
+// `err` receives 1 when an MMA completion wait ran out (the results are then invalid)
+void gemm(cudaStream_t st, unsigned* err, const __nv_bfloat16* A, int a_km, int lda, const __nv_bfloat16* B, int b_kn, int ldb, int M,
           int N, int K, const float* bias, float* out_f32, __nv_bfloat16* out_bf16, int ldc, int gelu) {
     GemmArgs g{A, B, M, N, K, lda, ldb, a_km, b_kn, bias, out_f32, out_bf16, ldc, gelu};
-    dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
-    k_gemm_bf16<<<grid, 128, 0, st>>>(g);
+    TSVD_CUDA(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M);
+    k_gemm_tc<<<grid, 128, kTcSmem, st>>>(g, err);
     TSVD_CUDA(cudaGetLastError());
 }
 
@@ -417,6 +533,7 @@ struct tsvd_encoder {
     tsvd::DevMem raw, mean, inv_std, std_;
     tsvd::DevMem users, h0, h0b, z1, h1b, z2, h2b, y, t, dy, dyb, dh2, dz2b, dh1, dz1b, dh0, part;
     tsvd::DevMem hist, inv_n;  // per batch user: rating and date-bin counts, 1 / history length
+    tsvd::DevMem tc_err;       // set by the tensor-core GEMM when an MMA wait ran out
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::string err;
@@ -459,11 +576,11 @@ void forward(tsvd_encoder* e, int n) {
                                               e->h0.as<float>(), e->h0b.as<__nv_bfloat16>(), e->hist.as<float>(),
                                               e->inv_n.as<float>());
     TSVD_CUDA(cudaGetLastError());
-    gemm(st, e->h0b.as<__nv_bfloat16>(), 0, kEmb, P(e, 3).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kEmb,
+    gemm(st, e->tc_err.as<unsigned>(), e->h0b.as<__nv_bfloat16>(), 0, kEmb, P(e, 3).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kEmb,
          P(e, 4).w.as<float>(), e->z1.as<float>(), e->h1b.as<__nv_bfloat16>(), kHid, 1);
-    gemm(st, e->h1b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kHid,
+    gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kHid,
          P(e, 6).w.as<float>(), e->z2.as<float>(), e->h2b.as<__nv_bfloat16>(), kHid, 1);
-    gemm(st, e->h2b.as<__nv_bfloat16>(), 0, kHid, P(e, 7).wb.as<__nv_bfloat16>(), 1, e->O, n, e->O, kHid,
+    gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 0, kHid, P(e, 7).wb.as<__nv_bfloat16>(), 1, e->O, n, e->O, kHid,
          P(e, 8).w.as<float>(), e->y.as<float>(), nullptr, e->O, 0);
 }
 
@@ -480,26 +597,26 @@ double backward(tsvd_encoder* e, int n) {
                               e->dyb.as<__nv_bfloat16>(), e->part.as<double>());
     TSVD_CUDA(cudaGetLastError());
     // layer 3
-    gemm(st, e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, O, kHid, O, n, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, O, kHid, O, n, nullptr,
          P(e, 7).g.as<float>(), nullptr, O, 0);
     k_colsum_f<<<(O + 127) / 128, 128, 0, st>>>(e->dy.as<float>(), n, O, P(e, 8).g.as<float>());
-    gemm(st, e->dyb.as<__nv_bfloat16>(), 0, O, P(e, 7).wb.as<__nv_bfloat16>(), 0, O, n, kHid, O, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->dyb.as<__nv_bfloat16>(), 0, O, P(e, 7).wb.as<__nv_bfloat16>(), 0, O, n, kHid, O, nullptr,
          e->dh2.as<float>(), nullptr, kHid, 0);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh2.as<float>(), e->z2.as<float>(), n * kHid,
                                                            e->dz2b.as<__nv_bfloat16>());
     // layer 2
-    gemm(st, e->h1b.as<__nv_bfloat16>(), 1, kHid, e->dz2b.as<__nv_bfloat16>(), 1, kHid, kHid, kHid, n, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 1, kHid, e->dz2b.as<__nv_bfloat16>(), 1, kHid, kHid, kHid, n, nullptr,
          P(e, 5).g.as<float>(), nullptr, kHid, 0);
     k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz2b.as<__nv_bfloat16>(), n, kHid, P(e, 6).g.as<float>());
-    gemm(st, e->dz2b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 0, kHid, n, kHid, kHid, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->dz2b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 0, kHid, n, kHid, kHid, nullptr,
          e->dh1.as<float>(), nullptr, kHid, 0);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh1.as<float>(), e->z1.as<float>(), n * kHid,
                                                            e->dz1b.as<__nv_bfloat16>());
     // layer 1
-    gemm(st, e->h0b.as<__nv_bfloat16>(), 1, kEmb, e->dz1b.as<__nv_bfloat16>(), 1, kHid, kEmb, kHid, n, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->h0b.as<__nv_bfloat16>(), 1, kEmb, e->dz1b.as<__nv_bfloat16>(), 1, kHid, kEmb, kHid, n, nullptr,
          P(e, 3).g.as<float>(), nullptr, kHid, 0);
     k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz1b.as<__nv_bfloat16>(), n, kHid, P(e, 4).g.as<float>());
-    gemm(st, e->dz1b.as<__nv_bfloat16>(), 0, kHid, P(e, 3).wb.as<__nv_bfloat16>(), 0, kHid, n, kEmb, kHid, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->dz1b.as<__nv_bfloat16>(), 0, kHid, P(e, 3).wb.as<__nv_bfloat16>(), 0, kHid, n, kEmb, kHid, nullptr,
          e->dh0.as<float>(), nullptr, kEmb, 0);
     // embeddings
     for (int k = 0; k < 3; ++k) TSVD_CUDA(cudaMemsetAsync(P(e, k).g.p, 0, P(e, k).n * 4, st));
@@ -526,6 +643,14 @@ void adamw_step(tsvd_encoder* e) {
                                                       p.decay ? e->wd : 0.0f, c1, c2,
                                                       p.wb.p ? p.wb.as<__nv_bfloat16>() : nullptr);
     TSVD_CUDA(cudaGetLastError());
+}
+
+// A tensor-core GEMM whose MMA wait ran out leaves its flag set: report it.
+void check_tc(tsvd_encoder* e) {
+    unsigned f = 0;
+    TSVD_CUDA(cudaMemcpyAsync(&f, e->tc_err.p, 4, cudaMemcpyDeviceToHost, e->stream));
+    TSVD_CUDA(cudaStreamSynchronize(e->stream));
+    if (f) throw Error(TSVD_ERR_TIMEOUT, "encoder GEMM: a tensor-core MMA did not complete within its wait limit");
 }
 
 void set_users(tsvd_encoder* e, const uint32_t* users, int n) {
@@ -649,6 +774,8 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->part.alloc(256 * 8);
         e->hist.alloc((size_t)B * (5 + s.T) * 4);
         e->inv_n.alloc((size_t)B * 4);
+        e->tc_err.alloc(4);
+        TSVD_CUDA(cudaMemset(e->tc_err.p, 0, 4));
         TSVD_CUDA(cudaDeviceSynchronize());
     });
     if (rc != TSVD_OK) {
@@ -689,6 +816,7 @@ int tsvd_encoder_train_epoch(tsvd_encoder* e, const uint32_t* users, uint64_t n,
             nb++;
         }
         TSVD_CUDA(cudaStreamSynchronize(e->stream));
+        check_tc(e);
         e->last_loss = nb ? tot / nb : 0.0;
         if (mean_loss) *mean_loss = e->last_loss;
     });
@@ -705,6 +833,7 @@ int tsvd_encoder_loss_grad(tsvd_encoder* e, const uint32_t* users, uint32_t n, d
         set_users(e, users, (int)n);
         forward(e, (int)n);
         const double l = backward(e, (int)n);
+        check_tc(e);
         if (loss) *loss = l;
     });
 }
@@ -720,6 +849,7 @@ int tsvd_encoder_forward(tsvd_encoder* e, const uint32_t* users, uint32_t n, flo
         forward(e, (int)n);
         TSVD_CUDA(cudaMemcpyAsync(out, e->y.p, (size_t)n * e->O * 4, cudaMemcpyDeviceToHost, e->stream));
         TSVD_CUDA(cudaStreamSynchronize(e->stream));
+        check_tc(e);
     });
 }
 
@@ -745,6 +875,7 @@ int tsvd_encoder_apply(tsvd_encoder* e, tsvd_model* m, const uint32_t* users, ui
             TSVD_CUDA(cudaGetLastError());
         }
         TSVD_CUDA(cudaStreamSynchronize(e->stream));
+        check_tc(e);
     });
 }
 

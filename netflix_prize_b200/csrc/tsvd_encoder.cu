@@ -427,8 +427,11 @@ __global__ void k_targets(DeviceState s, const uint32_t* __restrict__ users, int
 }
 
 // dY = 2 (y - t) / (n * O); per-block partial sums of the squared error.
-__global__ void k_mse(const float* __restrict__ y, const float* __restrict__ t, int total, float scale,
-                      float* __restrict__ dy, __nv_bfloat16* __restrict__ dyb, double* __restrict__ part) {
+// dyb is stored with leading dimension ldb >= O (16-byte rows for the GEMM's
+// vector staging).
+__global__ void k_mse(const float* __restrict__ y, const float* __restrict__ t, int total, int O, int ldb,
+                      float scale, float* __restrict__ dy, __nv_bfloat16* __restrict__ dyb,
+                      double* __restrict__ part) {
     __shared__ double sh[256];
     double acc = 0.0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
@@ -436,7 +439,7 @@ __global__ void k_mse(const float* __restrict__ y, const float* __restrict__ t, 
         acc += (double)d * d;
         const float g = 2.0f * d * scale;
         dy[e] = g;
-        dyb[e] = __float2bfloat16(g);
+        dyb[(size_t)(e / O) * ldb + e % O] = __float2bfloat16(g);
     }
     sh[threadIdx.x] = acc;
     __syncthreads();
@@ -473,7 +476,7 @@ __global__ void k_colsum(const __nv_bfloat16* __restrict__ x, int rows, int cols
 
 __global__ void k_adamw(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                         float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps, float wd, float c1,
-                        float c2, __nv_bfloat16* __restrict__ wb) {
+                        float c2, __nv_bfloat16* __restrict__ wb, uint32_t cols, uint32_t ldb) {
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const float gg = g[e];
         const float mm = b1 * m[e] + (1.0f - b1) * gg;
@@ -483,13 +486,15 @@ __global__ void k_adamw(float* __restrict__ w, const float* __restrict__ g, floa
         const float upd = (mm / c1) / (sqrtf(vv / c2) + eps) + wd * w[e];
         const float nw = w[e] - lr * upd;
         w[e] = nw;
-        if (wb) wb[e] = __float2bfloat16(nw);
+        if (wb) wb[(e / cols) * ldb + e % cols] = __float2bfloat16(nw);
     }
 }
 
-__global__ void k_f32_to_bf16(const float* __restrict__ x, size_t n, __nv_bfloat16* __restrict__ y) {
+// y keeps x's rows of `cols` values at leading dimension ldb
+__global__ void k_f32_to_bf16(const float* __restrict__ x, size_t n, __nv_bfloat16* __restrict__ y, uint32_t cols,
+                              uint32_t ldb) {
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-        y[e] = __float2bfloat16(x[e]);
+        y[(e / cols) * ldb + e % cols] = __float2bfloat16(x[e]);
 }
 
 // Writes de-standardised predictions into the model's user tables and resets
@@ -518,7 +523,8 @@ struct Param {
     std::string name;
     size_t n;
     bool decay;
-    DevMem w, g, m, v, wb;  // wb only for GEMM weights
+    uint32_t cols = 1, ldb = 1;  // row length and BF16 leading dimension (a multiple of 8) of wb
+    DevMem w, g, m, v, wb;       // wb only for GEMM weights
 };
 
 }  // namespace
@@ -527,6 +533,7 @@ struct Param {
 struct tsvd_encoder {
     const tsvd_model* model = nullptr;
     int O = 0;
+    int Op = 0;  // O rounded up to a multiple of 8: leading dimension of the BF16 copies of W3 and dY
     float lr = 1e-3f, wd = 1e-4f, b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     uint64_t step = 0;
     std::vector<tsvd::Param> params;  // e_item, e_rate, e_date, W1, b1, W2, b2, W3, b3
@@ -580,7 +587,7 @@ void forward(tsvd_encoder* e, int n) {
          P(e, 4).w.as<float>(), e->z1.as<float>(), e->h1b.as<__nv_bfloat16>(), kHid, 1);
     gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kHid,
          P(e, 6).w.as<float>(), e->z2.as<float>(), e->h2b.as<__nv_bfloat16>(), kHid, 1);
-    gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 0, kHid, P(e, 7).wb.as<__nv_bfloat16>(), 1, e->O, n, e->O, kHid,
+    gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 0, kHid, P(e, 7).wb.as<__nv_bfloat16>(), 1, e->Op, n, e->O, kHid,
          P(e, 8).w.as<float>(), e->y.as<float>(), nullptr, e->O, 0);
 }
 
@@ -593,14 +600,15 @@ double backward(tsvd_encoder* e, int n) {
     k_targets<<<(n * O + 255) / 256, 256, 0, st>>>(s, e->users.as<uint32_t>(), n, O, e->mean.as<float>(),
                                                    e->inv_std.as<float>(), e->t.as<float>());
     const int nb = 256;
-    k_mse<<<nb, 256, 0, st>>>(e->y.as<float>(), e->t.as<float>(), n * O, 1.0f / ((float)n * O), e->dy.as<float>(),
-                              e->dyb.as<__nv_bfloat16>(), e->part.as<double>());
+    const int Op = e->Op;
+    k_mse<<<nb, 256, 0, st>>>(e->y.as<float>(), e->t.as<float>(), n * O, O, Op, 1.0f / ((float)n * O),
+                              e->dy.as<float>(), e->dyb.as<__nv_bfloat16>(), e->part.as<double>());
     TSVD_CUDA(cudaGetLastError());
     // layer 3
-    gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, O, kHid, O, n, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, Op, kHid, O, n, nullptr,
          P(e, 7).g.as<float>(), nullptr, O, 0);
     k_colsum_f<<<(O + 127) / 128, 128, 0, st>>>(e->dy.as<float>(), n, O, P(e, 8).g.as<float>());
-    gemm(st, e->tc_err.as<unsigned>(), e->dyb.as<__nv_bfloat16>(), 0, O, P(e, 7).wb.as<__nv_bfloat16>(), 0, O, n, kHid, O, nullptr,
+    gemm(st, e->tc_err.as<unsigned>(), e->dyb.as<__nv_bfloat16>(), 0, Op, P(e, 7).wb.as<__nv_bfloat16>(), 0, Op, n, kHid, O, nullptr,
          e->dh2.as<float>(), nullptr, kHid, 0);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh2.as<float>(), e->z2.as<float>(), n * kHid,
                                                            e->dz2b.as<__nv_bfloat16>());
@@ -641,7 +649,7 @@ void adamw_step(tsvd_encoder* e) {
         k_adamw<<<grid_for(p.n), 256, 0, e->stream>>>(p.w.as<float>(), p.g.as<float>(), p.m.as<float>(),
                                                       p.v.as<float>(), p.n, e->lr, e->b1, e->b2, e->eps,
                                                       p.decay ? e->wd : 0.0f, c1, c2,
-                                                      p.wb.p ? p.wb.as<__nv_bfloat16>() : nullptr);
+                                                      p.wb.p ? p.wb.as<__nv_bfloat16>() : nullptr, p.cols, p.ldb);
     TSVD_CUDA(cudaGetLastError());
 }
 
@@ -674,16 +682,20 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->wd = weight_decay;
         const DeviceState& s = m->d;
         e->O = (int)s.F + 2;
+        e->Op = (e->O + 7) & ~7;
         TSVD_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
         e->raw.alloc(s.n_train);
         TSVD_CUDA(cudaMemcpy(e->raw.p, train_raw, s.n_train, cudaMemcpyHostToDevice));
         // parameters: Xavier-uniform matrices, N(0, 0.05) embeddings, zero biases
         ChaCha12Stream g(seed);
-        auto add = [&](const char* name, size_t n, bool decay, bool bf16, float scale, bool uniform) {
+        auto add = [&](const char* name, size_t n, bool decay, bool bf16, float scale, bool uniform,
+                       uint32_t cols = 1) {
             Param p;
             p.name = name;
             p.n = n;
             p.decay = decay;
+            p.cols = cols;
+            p.ldb = (cols + 7) & ~7u;
             std::vector<float> h(n, 0.0f);
             if (scale > 0) {
                 for (size_t k = 0; k < n; ++k) {
@@ -699,8 +711,10 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
             TSVD_CUDA(cudaMemset(p.m.p, 0, n * 4));
             TSVD_CUDA(cudaMemset(p.v.p, 0, n * 4));
             if (bf16) {
-                p.wb.alloc(n * 2);
-                k_f32_to_bf16<<<grid_for(n), 256>>>(p.w.as<float>(), n, p.wb.as<__nv_bfloat16>());
+                const size_t nb = n / cols * p.ldb;
+                p.wb.alloc(nb * 2);
+                TSVD_CUDA(cudaMemset(p.wb.p, 0, nb * 2));
+                k_f32_to_bf16<<<grid_for(n), 256>>>(p.w.as<float>(), n, p.wb.as<__nv_bfloat16>(), p.cols, p.ldb);
                 TSVD_CUDA(cudaGetLastError());
             }
             e->params.push_back(std::move(p));
@@ -716,11 +730,11 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         }
         add("e_rate", 5 * kEmb, false, false, 0.05f, false);
         add("e_date", (size_t)s.T * kEmb, false, false, 0.05f, false);
-        add("w1", (size_t)kEmb * kHid, true, true, std::sqrt(6.0f / (kEmb + kHid)), true);
+        add("w1", (size_t)kEmb * kHid, true, true, std::sqrt(6.0f / (kEmb + kHid)), true, kHid);
         add("b1", kHid, false, false, 0.0f, false);
-        add("w2", (size_t)kHid * kHid, true, true, std::sqrt(6.0f / (kHid + kHid)), true);
+        add("w2", (size_t)kHid * kHid, true, true, std::sqrt(6.0f / (kHid + kHid)), true, kHid);
         add("b2", kHid, false, false, 0.0f, false);
-        add("w3", (size_t)kHid * O, true, true, std::sqrt(6.0f / (kHid + O)), true);
+        add("w3", (size_t)kHid * O, true, true, std::sqrt(6.0f / (kHid + O)), true, (uint32_t)O);
         add("b3", (size_t)O, false, false, 0.0f, false);
         // target standardisation from the model's factors of the target users
         std::vector<float> mean(O, 0.0f), sd(O, 1.0f);
@@ -765,7 +779,7 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->y.alloc(B * O * 4);
         e->t.alloc(B * O * 4);
         e->dy.alloc(B * O * 4);
-        e->dyb.alloc(B * O * 2);
+        e->dyb.alloc(B * e->Op * 2);
         e->dh2.alloc(B * kHid * 4);
         e->dz2b.alloc(B * kHid * 2);
         e->dh1.alloc(B * kHid * 4);
@@ -910,7 +924,7 @@ int tsvd_encoder_set(tsvd_encoder* e, const char* name, const float* src, uint64
                 TSVD_CUDA(cudaMemcpy(p.w.p, src, count * 4, cudaMemcpyHostToDevice));
                 if (p.wb.p) {
                     k_f32_to_bf16<<<grid_for(p.n), 256, 0, e->stream>>>(p.w.as<float>(), p.n,
-                                                                       p.wb.as<__nv_bfloat16>());
+                                                                       p.wb.as<__nv_bfloat16>(), p.cols, p.ldb);
                     TSVD_CUDA(cudaStreamSynchronize(e->stream));
                 }
                 return;

@@ -362,11 +362,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_hog_batched(const DeviceState* 
 // src/tx.rs:391-418): train items in rating order, then pr items in pr order.
 // ---------------------------------------------------------------------------
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, const __nv_bfloat16* __restrict__ ybf);
+__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, const __nv_bfloat16* __restrict__ ybf,
+                                                              float* __restrict__ pyc);
 
 template <int VPL>
 __device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bfloat16* __restrict__ ybf, uint32_t u,
-                                             int lane);
+                                             int lane, float* __restrict__ pyc);
 
 // Batched ycache rebuild over (variant, user) pairs, variant-major.
 __global__ void __launch_bounds__(kThreads) k_rebuild_batched(const DeviceState* __restrict__ states,
@@ -378,29 +379,30 @@ __global__ void __launch_bounds__(kThreads) k_rebuild_batched(const DeviceState*
         const uint32_t mk = (uint32_t)(w / n_users), u = (uint32_t)(w - (uint64_t)mk * n_users);
         const DeviceState& s = states[mk];
         switch (s.Fs >> 5) {
-            case 1: rebuild_user<1>(s, nullptr, u, lane); break;
-            case 2: rebuild_user<2>(s, nullptr, u, lane); break;
-            case 3: rebuild_user<3>(s, nullptr, u, lane); break;
-            case 4: rebuild_user<4>(s, nullptr, u, lane); break;
-            case 5: rebuild_user<5>(s, nullptr, u, lane); break;
-            case 6: rebuild_user<6>(s, nullptr, u, lane); break;
-            case 7: rebuild_user<7>(s, nullptr, u, lane); break;
-            default: rebuild_user<8>(s, nullptr, u, lane); break;
+            case 1: rebuild_user<1>(s, nullptr, u, lane, nullptr); break;
+            case 2: rebuild_user<2>(s, nullptr, u, lane, nullptr); break;
+            case 3: rebuild_user<3>(s, nullptr, u, lane, nullptr); break;
+            case 4: rebuild_user<4>(s, nullptr, u, lane, nullptr); break;
+            case 5: rebuild_user<5>(s, nullptr, u, lane, nullptr); break;
+            case 6: rebuild_user<6>(s, nullptr, u, lane, nullptr); break;
+            case 7: rebuild_user<7>(s, nullptr, u, lane, nullptr); break;
+            default: rebuild_user<8>(s, nullptr, u, lane, nullptr); break;
         }
     }
 }
 
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, const __nv_bfloat16* __restrict__ ybf) {
+__global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, const __nv_bfloat16* __restrict__ ybf,
+                                                              float* __restrict__ pyc) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * kWarps;
     for (uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5); u < s.n_users; u += warps)
-        rebuild_user<VPL>(s, ybf, u, lane);
+        rebuild_user<VPL>(s, ybf, u, lane, pyc);
 }
 
 template <int VPL>
 __device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bfloat16* __restrict__ ybf, uint32_t u,
-                                             int lane) {
+                                             int lane, float* __restrict__ pyc) {
     constexpr int B = 8;  // rows in flight
     {
         float su[VPL];
@@ -443,6 +445,14 @@ __device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bf
         }
         Row<VPL>::store(s.ycache + (size_t)u * s.Fs, lane, su);
         if (lane == 0) s.ycache_bias[u] = sub;
+        if (pyc) {
+            // p_u + ycache_u, the user-side sum every item-stratum rating of u reads
+            float pu[VPL];
+            Row<VPL>::load_cg(s.ufeat + (size_t)u * s.Fs, lane, pu);
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) pu[v] = pu[v] + su[v];
+            Row<VPL>::store(pyc + (size_t)u * s.Fs, lane, pu);
+        }
     }
 }
 
@@ -460,9 +470,9 @@ void launch_hog_pass(tsvd_model* m, const EpochParams& p, const uint32_t* order)
 }
 
 template <int VPL>
-void launch_rebuild(tsvd_model* m, const __nv_bfloat16* ybf) {
+void launch_rebuild(tsvd_model* m, const __nv_bfloat16* ybf, float* pyc) {
     unsigned g = persistent_grid(k_rebuild_ycache<VPL>, 0);
-    k_rebuild_ycache<VPL><<<g, kThreads, 0, m->stream>>>(m->d, ybf);
+    k_rebuild_ycache<VPL><<<g, kThreads, 0, m->stream>>>(m->d, ybf, pyc);
     TSVD_CUDA(cudaGetLastError());
     m->launches++;
 }
@@ -496,18 +506,18 @@ void reset_counters(tsvd_model* m) {
 void rebuild_ycache(tsvd_model* m) {
     ProfScope ps(m, "rebuild_ycache");
     const int vpl = (int)(m->d.Fs / 32);
-    TSVD_DISPATCH(vpl, launch_rebuild<V>(m, nullptr));
+    TSVD_DISPATCH(vpl, launch_rebuild<V>(m, nullptr, nullptr));
     m->ycache_valid = true;
 }
 
 // Rebuild inside a stratified epoch: from the BF16 read copy of y in the
 // precision form, else from the FP32 master.
-void launch_rebuild_ycache(tsvd_model* m) {
+void launch_rebuild_ycache(tsvd_model* m, float* pyc) {
     ProfScope ps(m, "rebuild_ycache");
     const __nv_bfloat16* ybf =
         m->opts.precision >= TSVD_PREC_BF16_READ ? m->m_bf_yfeat.as<__nv_bfloat16>() : nullptr;
     const int vpl = (int)(m->d.Fs / 32);
-    TSVD_DISPATCH(vpl, launch_rebuild<V>(m, ybf));
+    TSVD_DISPATCH(vpl, launch_rebuild<V>(m, ybf, pyc));
     m->ycache_valid = true;
 }
 

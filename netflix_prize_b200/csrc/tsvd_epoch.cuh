@@ -84,9 +84,8 @@ struct Bf16Copies {
     const __nv_bfloat16* ifeat;   // [I, Fs]
     const __nv_bfloat16* qf0;     // [I, Fs] frequency-bin-0 rows of ifeat_freq
     const __nv_bfloat16* yfeat;   // [I, Fs]
-    const __nv_bfloat16* ufeat;   // [U, Fs]
+    const __nv_bfloat16* pyc;     // [U, Fs] p_u + ycache_u
     const __nv_bfloat16* ufeat2;  // [U, Fs]
-    const __nv_bfloat16* ycache;  // [U, Fs]
 };
 
 // Element (lane, v) of a bf16 row in Row<VPL>'s layout, widened to FP32.
@@ -136,6 +135,7 @@ unsigned persistent_grid(K kernel, size_t smem) {
 // tsvd_strat.cu
 void stratified_epoch(tsvd_model* m, const EpochParams& p);
 // tsvd_epoch.cu
-void launch_rebuild_ycache(tsvd_model* m);
+// pyc (optional, [U, Fs]) receives p_u + ycache_u for every user
+void launch_rebuild_ycache(tsvd_model* m, float* pyc = nullptr);
 
 }  // namespace tsvd

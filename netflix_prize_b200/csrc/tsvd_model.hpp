@@ -116,6 +116,8 @@ struct DeviceState {
     // stratified scratch
     float* g_user;   // [U, Fs] per-user NSVD1 gradient sum / norm
     float* e_user;   // [U]     per-user error sum / norm
+    float* pyc;      // [U, Fs] p_u + ycache_u for the item stratum; shares g_user's memory,
+                     //         which the delta sums have consumed by then
     // work lists
     const uint32_t* user_work;  // users in processing order
     const uint32_t* item_work;  // items in processing order
@@ -159,7 +161,7 @@ struct tsvd_model {
     tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
     tsvd::DevMem m_g_user, m_e_user, m_user_work, m_item_work, m_counters;
     // BF16 read copies (precision form)
-    tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_ufeat, m_bf_ufeat2, m_bf_ycache;
+    tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_pyc, m_bf_ufeat2;
     tsvd::DevMem m_chunk_lo, m_item_chunk0, m_chunk_part, m_chunk_epart;
     tsvd::DevMem m_perm;          // [U] epoch order upload buffer
     tsvd::DevMem m_scratch;       // predict / rmse scratch

@@ -489,9 +489,8 @@ void setup_params(tsvd_model* m) {
             m->m_bf_yfeat.alloc((size_t)I * Fs * 2);
         }
         if (m->opts.precision >= TSVD_PREC_BF16_READ_ALL) {
-            m->m_bf_ufeat.alloc((size_t)U * Fs * 2);
+            m->m_bf_pyc.alloc((size_t)U * Fs * 2);
             m->m_bf_ufeat2.alloc((size_t)U * Fs * 2);
-            m->m_bf_ycache.alloc((size_t)U * Fs * 2);
         }
         s.ubias = m->m_ubias.as<float>(); s.ibias = m->m_ibias.as<float>();
         s.ufeat = m->m_ufeat.as<float>(); s.ufeat2 = m->m_ufeat2.as<float>();
@@ -507,6 +506,7 @@ void setup_params(tsvd_model* m) {
         s.cu = m->m_cu.as<float>(); s.cut = m->m_cut.as<float>();
         s.thresholds = m->m_thresholds.as<float>();
         s.g_user = m->m_g_user.as<float>(); s.e_user = m->m_e_user.as<float>();
+        s.pyc = s.g_user;
         s.counters = m->m_counters.as<uint32_t>();
         if (c.has_ordinal_head) {
             TSVD_CUDA(cudaMemcpyAsync(m->m_thresholds.p, c.ordinal_head.th_init, 16, cudaMemcpyHostToDevice, st));

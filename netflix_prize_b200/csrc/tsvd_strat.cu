@@ -14,6 +14,7 @@
 // reads are gathered as BF16 (item rows q_i, q^f_{i,0} and y_j; optionally
 // the user rows p_u, p2_u, ycache_u of the item stratum) and widened to FP32
 // for accumulation; masters stay FP32 and are the only tables written.
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -291,31 +292,50 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
 // Item stratum. An item's ratings form a serial chain (every update feeds the
 // next dot product), and the most-rated items carry ~0.5% of all ratings
 // each, so the chain of the hottest item bounds the pass. Items with >= kHeavy
-// ratings get a whole CTA, warp-specialised: warps 1..7 gather the user rows of
-// the next round of kRound ratings and fold them into
-// pe = (p_u + ycache_u) + dev * p2_u plus the rating's bias scalars in shared
-// memory (double-buffered rounds, one __syncthreads per round), while warp 0
-// runs the chain from shared memory only. Lighter items take one warp each,
-// with the next rating's rows prefetched into registers.
+// ratings get a whole CTA of kCW + kPW warps, in rounds of kRound ratings:
+//   producers (kPW warps) gather the next round's user rows into
+//     pe = (p_u + ycache_u) + dev * p2_u plus the rating's bias scalars,
+//     form the round's Gram matrix on the tensor cores and from it the
+//     round's lower-triangular system (everything about the round that does
+//     not depend on the item's current rows);
+//   consumers (kCW warps, each owning every kCW-th 32-column stripe of q and
+//     of the q^f rows) take the dots with the item's rows, warp 0 solves the
+//     system for the round's errors, and all of them apply the closed-form
+//     updates to their stripes.
+// Rounds are double-buffered with one __syncthreads per round. Lighter items
+// take one warp each, with the next rating's rows prefetched into registers.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kHeavy = 1024;
 constexpr int kRound = 32;  // ratings per buffered round
-constexpr uint32_t kGramStride = kRound + 1;  // padded rows of the per-round Gram matrix
+constexpr uint32_t kMS = kRound + 1;  // padded row stride of the round's system M
+constexpr int kCW = 4;                // consumer warps
+constexpr int kPW = 8;                // producer warps
+constexpr int kItemThreads = (kCW + kPW) * 32;
+constexpr int kVecs = 9;              // per-rating vectors of a round
+// BF16 rows of the Gram operands: Fs values + 16 bytes, so that the eight
+// 16-byte row segments an ldmatrix reads fall in distinct bank groups
+__host__ __device__ constexpr uint32_t hl_pitch(uint32_t Fs) { return Fs * 2 + 16; }
+static_assert(kPW * 4 == kRound, "each producer warp stages four of the round's ratings");
 
-// x = hi + lo with hi, lo in TF32 (round to nearest, ties away from zero).
-__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
-    const float rest = x - __uint_as_float(hi);
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rest));
-}
-
-// d (16x8, FP32) += a (16x8, TF32, row-major) . b (8x8, TF32, column-major)
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+// Shared-memory layout of the item pass, in floats (every offset a multiple of 4).
+struct ItemSmem {
+    uint32_t qfs, qsh, buf, hl, mbuf, vec, pd, sv, ap, pw, total;
+};
+__host__ __device__ inline ItemSmem item_smem(uint32_t Fs, uint32_t NF) {
+    ItemSmem L;
+    uint32_t o = 0;
+    L.qfs = o;  o += NF * (Fs + 4);             // the item's q^f rows, padded
+    L.qsh = o;  o += Fs;                        // q at the round's start
+    L.buf = o;  o += 2 * kRound * (Fs + 4);     // two rounds of pe rows + {bu_t, cu_t, res, key}
+    L.hl = o;   o += 2 * kRound * (Fs / 2 + 4); // BF16 high and low parts of the produced round's pe rows
+    L.mbuf = o; o += 2 * kRound * kMS;          // two rounds of the system M (row j: M_j,i)
+    L.vec = o;  o += 2 * kVecs * kRound;        // two rounds of per-rating weights
+    L.pd = o;   o += kCW * 2 * kRound;          // consumers' partial dots
+    L.sv = o;   o += 4 * kRound;                // the round's update weights (q, q^f, biases)
+    L.ap = o;   o += 4 * kRound;                // per rating {w_q, w_f, decay, bin | previous << 8}
+    L.pw = o;   o += 2 * 36;                    // a_i^n, a_f^n for n = 0..kRound
+    L.total = o;
+    return L;
 }
 
 struct ItemState {
@@ -351,17 +371,16 @@ __device__ __forceinline__ void user_scalars(const DeviceState& s, const Rec& r,
     cu_t = __ldg(s.cu + u) + (hud ? __ldg(s.cut + r.ud) : 0.0f);
 }
 
+// The user-side rows of a by-item rating: p_u + ycache_u and p2_u.
 template <int VPL, bool BF>
-__device__ __forceinline__ void user_rows(const DeviceState& s, const Bf16Copies& bf, uint32_t u, int lane,
-                                          float (&pu)[VPL], float (&p2)[VPL], float (&yc)[VPL]) {
+__device__ __forceinline__ void pe_rows(const DeviceState& s, const Bf16Copies& bf, uint32_t u, int lane,
+                                        float (&pyc)[VPL], float (&p2)[VPL]) {
     if constexpr (BF) {
-        row_load_bf16<VPL>(bf.ufeat + (size_t)u * s.Fs, lane, pu);
+        row_load_bf16<VPL>(bf.pyc + (size_t)u * s.Fs, lane, pyc);
         row_load_bf16<VPL>(bf.ufeat2 + (size_t)u * s.Fs, lane, p2);
-        row_load_bf16<VPL>(bf.ycache + (size_t)u * s.Fs, lane, yc);
     } else {
-        Row<VPL>::load_nc(s.ufeat + (size_t)u * s.Fs, lane, pu);
+        Row<VPL>::load_nc(s.pyc + (size_t)u * s.Fs, lane, pyc);
         Row<VPL>::load_nc(s.ufeat2 + (size_t)u * s.Fs, lane, p2);
-        Row<VPL>::load_nc(s.ycache + (size_t)u * s.Fs, lane, yc);
     }
 }
 
@@ -417,14 +436,14 @@ __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf1
         const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
         Rec mine{};
         if (lane < (int)cnt) mine = load_rec(s.irec + base + lane);
-        float pn[VPL], p2n[VPL], ycn[VPL];
-        user_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, 0)), lane, pn, p2n, ycn);
+        float pn[VPL], p2n[VPL];
+        pe_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, 0)), lane, pn, p2n);
         for (uint32_t j = 0; j < cnt; ++j) {
             const Rec r = shfl_rec(mine, j);
             float pe[VPL];
 #pragma unroll
-            for (int v = 0; v < VPL; ++v) pe[v] = (pn[v] + ycn[v]) + r.dev * p2n[v];
-            if (j + 1 < cnt) user_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, j + 1)), lane, pn, p2n, ycn);
+            for (int v = 0; v < VPL; ++v) pe[v] = pn[v] + r.dev * p2n[v];
+            if (j + 1 < cnt) pe_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, j + 1)), lane, pn, p2n);
             float bu_t, cu_t;
             user_scalars(s, r, bu_t, cu_t);
             const uint32_t tb = rec_tbin(r.key), fb = rec_fbin(r.key);
@@ -440,18 +459,97 @@ __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf1
     store_item_state(s, i, lane, st);
 }
 
+// x = hi + lo + r with hi, lo in BF16 (round to nearest even), |r| <= 2^-17 |x|.
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    hi = __float2bfloat16_rn(x);
+    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// One staged rating: its FP32 pe row (for the consumers) and the BF16 high and
+// low parts of it (the Gram operands), each element split once.
+template <int VPL>
+__device__ __forceinline__ void stage_row(float* row, uint8_t* hi_row, uint8_t* lo_row, int lane,
+                                          const float (&pe)[VPL]) {
+    if constexpr (VPL % 4 == 0) {
+#pragma unroll
+        for (int c = 0; c < VPL / 4; ++c) {
+            const int col = c * 128 + lane * 4;
+            const float4 x = make_float4(pe[4 * c], pe[4 * c + 1], pe[4 * c + 2], pe[4 * c + 3]);
+            *reinterpret_cast<float4*>(row + col) = x;
+            __nv_bfloat16 h[4], l[4];
+            split_bf16(x.x, h[0], l[0]);
+            split_bf16(x.y, h[1], l[1]);
+            split_bf16(x.z, h[2], l[2]);
+            split_bf16(x.w, h[3], l[3]);
+            *reinterpret_cast<uint2*>(hi_row + 2 * col) = *reinterpret_cast<const uint2*>(h);
+            *reinterpret_cast<uint2*>(lo_row + 2 * col) = *reinterpret_cast<const uint2*>(l);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+            const int col = Row<VPL>::elem(lane, v);
+            row[col] = pe[v];
+            __nv_bfloat16 h, l;
+            split_bf16(pe[v], h, l);
+            reinterpret_cast<__nv_bfloat16*>(hi_row)[col] = h;
+            reinterpret_cast<__nv_bfloat16*>(lo_row)[col] = l;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], uint32_t addr) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+
+// d (16x8, FP32) += a (16x16, BF16, row-major) . b (16x8, BF16, column-major)
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
 template <int VPL, bool BF>
-__global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochParams p, Bf16Copies bf) {
-    extern __shared__ float smem[];
+__global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, EpochParams p, Bf16Copies bf) {
+    extern __shared__ __align__(16) float smem[];
     __shared__ uint32_t sh_k;
+    static_assert(kCW == 4, "the consumers' partial dots are summed as (0 + 1) + (2 + 3)");
+    constexpr int CPL = (VPL + kCW - 1) / kCW;  // 32-column stripes per consumer warp
+    constexpr int kChunk = 8;                   // ratings per step of the consumers' apply
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t Fs = s.Fs, NF = s.NF;
-    const uint32_t stride = Fs + 4;       // one staged rating: pe row + {bu_t, cu_t, res, key}
-    const uint32_t qs = Fs + 4;           // padded q^f row stride (rows of different bins in distinct banks)
-    float* qfs = smem;                    // [NF][qs]
-    float* qsh = qfs + (size_t)NF * qs;   // [Fs] q row of the current round
-    float* buf = qsh + Fs;                // [2][kRound][stride]
-    float* gram = buf + 2ull * kRound * stride;  // [2][kRound][kGramStride]
+    const uint32_t Fs = s.Fs, NF = s.NF, NS = Fs / 32;
+    const uint32_t stride = Fs + 4;  // one staged rating: pe row + {bu_t, cu_t, res, key}
+    const uint32_t qs = Fs + 4;      // padded q^f row stride
+    const ItemSmem L = item_smem(Fs, NF);
+    float* qfs = smem + L.qfs;
+    float* qsh = smem + L.qsh;
+    float* buf = smem + L.buf;
+    uint8_t* hl = reinterpret_cast<uint8_t*>(smem + L.hl);
+    const uint32_t hp = hl_pitch(Fs);
+    float* mbuf = smem + L.mbuf;
+    float* vec = smem + L.vec;
+    float* pd = smem + L.pd;
+    float* sv = smem + L.sv;
+    float4* ap = reinterpret_cast<float4*>(smem + L.ap);
+    float* apow = smem + L.pw;  // apow[n] = a_i^n, fpow[n] = a_f^n (products in order)
+    float* fpow = apow + 36;
+    // update factors: x - lr (g + reg x) = a x - lr g
+    const float a_i = 1.0f - p.lr_i * p.reg_i, a_f = 1.0f - p.lr_iqf * p.reg_iqf;
+    if (threadIdx.x == 0) {
+        float x = 1.0f, y = 1.0f;
+        for (int e = 0; e <= kRound; ++e) {
+            apow[e] = x;
+            fpow[e] = y;
+            x *= a_i;
+            y *= a_f;
+        }
+    }
+    const float gb = s.gbias;
     for (;;) {
         if (threadIdx.x == 0) sh_k = atomicAdd(&s.counters[2], 1u);
         __syncthreads();
@@ -476,109 +574,160 @@ __global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochP
             qfs[(e / Fs) * qs + e % Fs] = __ldcg(s.ifeat_freq + (size_t)i * NF * Fs + e);
         const uint64_t n = b - a;
         const uint32_t rounds = (uint32_t)((n + kRound - 1) / kRound);
-        float q[VPL];
+        float qv[CPL];  // consumer warp c: q columns 32 (c + kCW t) + lane
         ItemState st{};
-        if (warp == 0) {
-            Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
-            st = load_item_state(s, i, lane);
+        if (warp < kCW) {
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const uint32_t sc = warp + kCW * t;
+                qv[t] = sc < NS ? __ldcg(s.ifeat + (size_t)i * Fs + 32 * sc + lane) : 0.0f;
+            }
+            if (warp == 0) st = load_item_state(s, i, lane);
         }
         auto round_len = [&](uint32_t r) -> uint32_t {
             const uint64_t left = n - (uint64_t)r * kRound;
             return (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
         };
+        // Producers hold the next round's records (one per lane) and, on the
+        // lanes whose rows they stage, its user-side scalars, loaded a round
+        // ahead so that their latency overlaps the wait for the consumers.
+        Rec nx{};
+        float nbu = 0.0f, ncu = 0.0f;
+        auto prefetch = [&](uint32_t r) {
+            const int pw = warp - kCW;
+            const bool valid = lane < (int)round_len(r);
+            nx = Rec{};
+            nbu = ncu = 0.0f;
+            if (valid) nx = load_rec(s.irec + a + (uint64_t)r * kRound + lane);
+            if (valid && (lane & (kPW - 1)) == pw) user_scalars(s, nx, nbu, ncu);
+        };
+        // Producer warp pw: round r's pe rows pw, pw + 8, pw + 16, pw + 24 and
+        // their scalars, then (pw < 6) a Gram tile and the entries of the
+        // round's system M that it holds, or (pw == 6) the per-rating weights.
         auto produce = [&](uint32_t r) {
+            const int pw = warp - kCW;
             float* dst = buf + (size_t)(r & 1) * kRound * stride;
-            const uint64_t r0 = a + (uint64_t)r * kRound;
+            float* Mb = mbuf + (size_t)(r & 1) * kRound * kMS;
+            float* V = vec + (size_t)(r & 1) * kVecs * kRound;
             const uint32_t m = round_len(r);
-            // the round's records and user-side scalars, one rating per lane
-            Rec mine{};
-            float bu_l = 0.0f, cu_l = 0.0f;
-            if ((uint32_t)lane < m) {
-                mine = load_rec(s.irec + r0 + lane);
-                user_scalars(s, mine, bu_l, cu_l);
+            const bool valid = lane < (int)m;
+            const Rec mine = nx;
+            if ((lane & (kPW - 1)) == pw) {
+                float* row = dst + (size_t)lane * stride;
+                row[Fs] = nbu;
+                row[Fs + 1] = ncu;
+                row[Fs + 2] = mine.res;
+                row[Fs + 3] = __uint_as_float(mine.key);
             }
-            auto put = [&](uint32_t j, const float (&pu)[VPL], const float (&p2)[VPL], const float (&yc)[VPL]) {
-                const float dev = __shfl_sync(kFull, mine.dev, j), bu = __shfl_sync(kFull, bu_l, j);
-                const float cu = __shfl_sync(kFull, cu_l, j), res = __shfl_sync(kFull, mine.res, j);
-                const uint32_t key = __shfl_sync(kFull, mine.key, j);
-                float* row = dst + (size_t)j * stride;
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) row[Row<VPL>::elem(lane, v)] = (pu[v] + yc[v]) + dev * p2[v];
-                if (lane == 0) {
-                    row[Fs] = bu;
-                    row[Fs + 1] = cu;
-                    row[Fs + 2] = res;
-                    row[Fs + 3] = __uint_as_float(key);
-                }
-            };
-            // user rows of two ratings in flight per warp
-            for (uint32_t j0 = warp - 1; j0 < m; j0 += 2 * (kWarps - 1)) {
-                const uint32_t j1 = j0 + (kWarps - 1);
-                const bool two = j1 < m;
+            // two ratings' user rows in flight; rows m..31 of a partial round are zero
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t j0 = pw + 16 * h, j1 = j0 + kPW;
                 const uint32_t u0 = rec_id(__shfl_sync(kFull, mine.key, j0));
-                const uint32_t u1 = rec_id(__shfl_sync(kFull, mine.key, two ? j1 : j0));
-                float pa[VPL], p2a[VPL], yca[VPL], pb[VPL], p2b[VPL], ycb[VPL];
-                user_rows<VPL, BF>(s, bf, u0, lane, pa, p2a, yca);
-                if (two) user_rows<VPL, BF>(s, bf, u1, lane, pb, p2b, ycb);
-                put(j0, pa, p2a, yca);
-                if (two) put(j1, pb, p2b, ycb);
-            }
-            // rows m..31 of a partial round are zero (finite values for the
-            // consumer's unconditional loops)
-            for (uint32_t j = m + warp - 1; j < (uint32_t)kRound; j += kWarps - 1) {
-                float* row = dst + (size_t)j * stride;
-                for (uint32_t e = lane; e < stride; e += 32) row[e] = 0.0f;
+                const uint32_t u1 = rec_id(__shfl_sync(kFull, mine.key, j1));
+                const float d0 = __shfl_sync(kFull, mine.dev, j0), d1 = __shfl_sync(kFull, mine.dev, j1);
+                float x0[VPL], y0[VPL], x1[VPL], y1[VPL];
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) x0[v] = y0[v] = x1[v] = y1[v] = 0.0f;
+                if (j0 < m) pe_rows<VPL, BF>(s, bf, u0, lane, x0, y0);
+                if (j1 < m) pe_rows<VPL, BF>(s, bf, u1, lane, x1, y1);
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) {
+                    x0[v] = x0[v] + d0 * y0[v];
+                    x1[v] = x1[v] + d1 * y1[v];
+                }
+                stage_row<VPL>(dst + (size_t)j0 * stride, hl + (size_t)j0 * hp, hl + (size_t)(kRound + j0) * hp, lane, x0);
+                stage_row<VPL>(dst + (size_t)j1 * stride, hl + (size_t)j1 * hp, hl + (size_t)(kRound + j1) * hp, lane, x1);
             }
             // all rows of the round are in place before the Gram products
-            asm volatile("bar.sync 1, %0;" ::"r"((kWarps - 1) * 32) : "memory");
-            // G = PE PE^T for the round's ratings, on the tensor cores: TF32
-            // operands split into high and low parts, three products per
-            // tile (error near FP32's). Producer warp w takes tile w - 1 of
-            // the six 16x8 tiles that hold the pairs k < j.
-            const int tile = warp - 1;
-            if (tile < 6) {
-                float* gm = gram + (size_t)(r & 1) * kRound * kGramStride;
-                const int mt = tile < 4 ? 0 : 1, nt = tile < 4 ? tile : tile - 2;
+            asm volatile("bar.sync 2, %0;" ::"r"(kPW * 32) : "memory");
+            const uint32_t fbl = rec_fbin(mine.key);
+            // the round's ratings of each frequency bin (valid ratings only)
+            const unsigned same = __match_any_sync(kFull, valid ? fbl : 64u + (uint32_t)lane);
+            if (pw < 6) {
+                // G = PE PE^T on the tensor cores, from BF16 high and low
+                // parts of pe (three products: error ~2^-16 of |pe_i||pe_j|).
+                // Tile pw of the six 16x8 tiles (rows x columns) that hold
+                // every pair row < column.
+                const int mt = pw < 4 ? 0 : 1, nt = pw < 4 ? pw : pw - 2;
                 const int gid = lane >> 2, tig = lane & 3;
-                const float* A0 = dst + (size_t)(mt * 16 + gid) * stride;
-                const float* A1 = A0 + 8 * (size_t)stride;
-                const float* B0 = dst + (size_t)(nt * 8 + gid) * stride;
-                // independent accumulators: the three split products and
-                // even/odd k-steps run as separate MMA chains
+                // ldmatrix row addresses: A (16x16) as four 8x8 matrices
+                // (rows 0-7 | 8-15) x (k 0-7 | 8-15); B's high and low parts
+                // (8 pe rows x k 0-7 | 8-15) in one x4
+                const uint32_t hl_s = smem_u32(hl);
+                const int ar = mt * 16 + (lane & 7) + 8 * ((lane >> 3) & 1), ak = 8 * (lane >> 4);
+                const uint32_t a_hi = hl_s + (uint32_t)(ar * hp + 2 * ak);
+                const uint32_t a_lo = a_hi + (uint32_t)(kRound * hp);
+                const int br = nt * 8 + (lane & 7), bk = 8 * ((lane >> 3) & 1);
+                const uint32_t b_hl = hl_s + (uint32_t)(((lane >> 4) * kRound + br) * hp + 2 * bk);
                 float d[6][4] = {};
 #pragma unroll 2
-                for (uint32_t k0 = 0; k0 < Fs; k0 += 16) {
+                for (uint32_t k0 = 0; k0 < Fs; k0 += 32) {
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const uint32_t kk = k0 + 8 * h;
-                        uint32_t ah[4], al[4], bh[2], bl[2];
-                        split_tf32(A0[kk + tig], ah[0], al[0]);
-                        split_tf32(A1[kk + tig], ah[1], al[1]);
-                        split_tf32(A0[kk + tig + 4], ah[2], al[2]);
-                        split_tf32(A1[kk + tig + 4], ah[3], al[3]);
-                        split_tf32(B0[kk + tig], bh[0], bl[0]);
-                        split_tf32(B0[kk + tig + 4], bh[1], bl[1]);
-                        mma_tf32(d[3 * h], al, bh);
-                        mma_tf32(d[3 * h + 1], ah, bl);
-                        mma_tf32(d[3 * h + 2], ah, bh);
+                    for (int hh = 0; hh < 2; ++hh) {
+                        const uint32_t kb = 2 * (k0 + 16 * hh);
+                        uint32_t ah[4], al[4], bb[4];
+                        ldmatrix_x4(ah, a_hi + kb);
+                        ldmatrix_x4(al, a_lo + kb);
+                        ldmatrix_x4(bb, b_hl + kb);
+                        const uint32_t bh[2] = {bb[0], bb[1]}, bl[2] = {bb[2], bb[3]};
+                        mma_bf16(d[3 * hh], al, bh);
+                        mma_bf16(d[3 * hh + 1], ah, bl);
+                        mma_bf16(d[3 * hh + 2], ah, bh);
                     }
                 }
+                // The round's errors solve err = C - M err with M unit lower
+                // triangular: M_ji (i < j) is the effect of err_i on rating j
+                // through q (a_i^(j-1-i) G_ij), the q^f row of a shared bin
+                // (a_f^(same-bin ratings between) G_ij) and the item biases.
+                // This lane's four entries (i, j) give M_ji and M_ij = 0.
 #pragma unroll
-                for (int e = 0; e < 4; ++e) d[0][e] = ((d[0][e] + d[1][e]) + (d[3][e] + d[4][e])) + (d[2][e] + d[5][e]);
-                float* g0 = gm + (size_t)(mt * 16 + gid) * kGramStride + nt * 8 + 2 * tig;
-                g0[0] = d[0][0];
-                g0[1] = d[0][1];
-                g0[8 * kGramStride] = d[0][2];
-                g0[8 * kGramStride + 1] = d[0][3];
+                for (int e = 0; e < 4; ++e) {
+                    const float g = ((d[0][e] + d[1][e]) + (d[3][e] + d[4][e])) + (d[2][e] + d[5][e]);
+                    const int ii = mt * 16 + gid + 8 * (e >> 1), jj = nt * 8 + 2 * tig + (e & 1);
+                    const uint32_t ki = __shfl_sync(kFull, mine.key, ii), kj = __shfl_sync(kFull, mine.key, jj);
+                    const unsigned samej = __shfl_sync(kFull, same, jj);
+                    if (ii < jj) {
+                        float v = 0.0f;
+                        if (jj < (int)m) {
+                            const float cui = dst[(size_t)ii * stride + Fs + 1], cuj = dst[(size_t)jj * stride + Fs + 1];
+                            const bool same_f = rec_fbin(ki) == rec_fbin(kj), same_t = rec_tbin(ki) == rec_tbin(kj);
+                            const float bias_lr = p.lr_ib + (same_t ? p.lr_ti : 0.0f) + (same_f ? p.lr_ibf : 0.0f);
+                            const unsigned between = ((1u << jj) - 1u) & ~((2u << ii) - 1u);
+                            v = cuj * cui * bias_lr + p.lr_i * apow[jj - 1 - ii] * g +
+                                (same_f ? p.lr_iqf * fpow[__popc(samej & between)] * g : 0.0f);
+                        }
+                        Mb[(size_t)jj * kMS + ii] = v;
+                        Mb[(size_t)ii * kMS + jj] = 0.0f;
+                    } else if (ii == jj) {
+                        Mb[(size_t)ii * kMS + ii] = 0.0f;
+                    }
+                }
+            } else if (pw == 6) {
+                // per-rating weights of the round (j = lane)
+                const unsigned below = (1u << lane) - 1u, above = ~((2u << lane) - 1u);
+                const unsigned earlier = same & below;
+                V[lane] = apow[lane];                                       // a_i^j
+                V[kRound + lane] = fpow[__popc(earlier)];                   // a_f^(earlier ratings of the bin)
+                V[2 * kRound + lane] = valid ? apow[valid ? m - 1 - lane : 0] : 0.0f;  // a_i^(m-1-j)
+                V[3 * kRound + lane] = fpow[__popc(same & above)];          // a_f^(later ratings of the bin)
+                // the first rating of a bin applies the decay of all its ratings to the bin's row
+                V[4 * kRound + lane] = (valid && earlier == 0u) ? fpow[__popc(same)] : 1.0f;
+                V[5 * kRound + lane] = __uint_as_float(fbl);
+                if (lane == 0) V[6 * kRound] = apow[m];                     // a_i^m
+                // the previous rating of the same bin in the round, or -1
+                V[7 * kRound + lane] = __int_as_float(earlier ? 31 - __clz((int)earlier) : -1);
+                V[8 * kRound + lane] = __uint_as_float(rec_tbin(mine.key));
             }
+            if (r + 1 < rounds) prefetch(r + 1);
         };
-        if (warp > 0) produce(0);
+        if (warp >= kCW) {
+            prefetch(0);
+            produce(0);
+        }
         __syncthreads();
-        const float gb = s.gbias;
-        // update factors: x - lr (g + reg x) = a x - lr g
-        const float a_i = 1.0f - p.lr_i * p.reg_i, a_f = 1.0f - p.lr_iqf * p.reg_iqf;
         for (uint32_t r = 0; r < rounds; ++r) {
-            if (warp > 0) {
+            if (warp >= kCW) {
                 if (r + 1 < rounds) produce(r + 1);
             } else {
                 // Lookahead over the round's m ratings (all of one item): with
@@ -587,94 +736,143 @@ __global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochP
                 //   q_k . pe_k = a_i^k (q_0 . pe_k) - lr_i sum_{j<k} a_i^(k-1-j) err_j G_jk
                 // and likewise for the q^f row of pe_k's frequency bin over the
                 // earlier ratings of the same bin. The dots with q_0 are taken
-                // once per round; the serial chain is then scalar per rating,
-                // and the round's updates are applied in closed form,
+                // once per round; the round's updates are applied in closed form,
                 //   q_m = a_i^m q_0 - lr_i sum_k a_i^(m-1-k) err_k pe_k.
-                // Rows m..31 of a partial round are zero.
                 const float* src = buf + (size_t)(r & 1) * kRound * stride;
-                const float* gm = gram + (size_t)(r & 1) * kRound * kGramStride;
+                const float* Mb = mbuf + (size_t)(r & 1) * kRound * kMS;
+                const float* V = vec + (size_t)(r & 1) * kVecs * kRound;
                 const uint32_t m = round_len(r);
                 const float* myrow = src + (size_t)lane * stride;
-                const float bu_t = myrow[Fs], cu_t = myrow[Fs + 1], res = myrow[Fs + 2];
-                const uint32_t key = __float_as_uint(myrow[Fs + 3]);
-                const uint32_t tb = rec_tbin(key), fb = rec_fbin(key);
-                // this lane's dots with q_0 and q^f_0[fb]: the round's q row
-                // goes to shared memory, and each lane walks its own pe row
+                const uint32_t keyl = __float_as_uint(myrow[Fs + 3]);
+                const uint32_t fbl = rec_fbin(keyl);
+                // partial dots of pe_lane with q_0 and q^f_0[fb] over this warp's stripes
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) qsh[Row<VPL>::elem(lane, v)] = q[v];
+                for (int t = 0; t < CPL; ++t) {
+                    const uint32_t sc = warp + kCW * t;
+                    if (sc < NS) qsh[32 * sc + lane] = qv[t];
+                }
                 __syncwarp();
-                float sq, sf;
                 {
-                    const float4* x4 = reinterpret_cast<const float4*>(myrow);
-                    const float4* y4 = reinterpret_cast<const float4*>(qsh);
-                    const float4* z4 = reinterpret_cast<const float4*>(qfs + (size_t)fb * qs);
                     float s0 = 0.0f, s1 = 0.0f, e0 = 0.0f, e1 = 0.0f;
-#pragma unroll 4
-                    for (uint32_t k4 = 0; k4 < Fs / 4; ++k4) {
-                        const float4 x = x4[k4], y = y4[k4], z = z4[k4];
-                        s0 = fmaf(x.x, y.x, s0);
-                        s1 = fmaf(x.y, y.y, s1);
-                        s0 = fmaf(x.z, y.z, s0);
-                        s1 = fmaf(x.w, y.w, s1);
-                        e0 = fmaf(x.x, z.x, e0);
-                        e1 = fmaf(x.y, z.y, e1);
-                        e0 = fmaf(x.z, z.z, e0);
-                        e1 = fmaf(x.w, z.w, e1);
+#pragma unroll
+                    for (int t = 0; t < CPL; ++t) {
+                        const uint32_t sc = warp + kCW * t;
+                        if (sc < NS) {
+                            const float4* x4 = reinterpret_cast<const float4*>(myrow + 32 * sc);
+                            const float4* y4 = reinterpret_cast<const float4*>(qsh + 32 * sc);
+                            const float4* z4 = reinterpret_cast<const float4*>(qfs + (size_t)fbl * qs + 32 * sc);
+#pragma unroll
+                            for (int k4 = 0; k4 < 8; ++k4) {
+                                const float4 x = x4[k4], y = y4[k4], z = z4[k4];
+                                s0 = fmaf(x.x, y.x, s0);
+                                s1 = fmaf(x.y, y.y, s1);
+                                s0 = fmaf(x.z, y.z, s0);
+                                s1 = fmaf(x.w, y.w, s1);
+                                e0 = fmaf(x.x, z.x, e0);
+                                e1 = fmaf(x.y, z.y, e1);
+                                e0 = fmaf(x.z, z.z, e0);
+                                e1 = fmaf(x.w, z.w, e1);
+                            }
+                        }
                     }
-                    sq = s0 + s1;  // q_0 . pe_lane
-                    sf = e0 + e1;  // qf_0[fb] . pe_lane
+                    pd[(2 * warp) * kRound + lane] = s0 + s1;
+                    pd[(2 * warp + 1) * kRound + lane] = e0 + e1;
                 }
-                // The round's errors solve a unit lower-triangular system
-                // err = C - M err: C_j holds everything known at the round's
-                // start, M_ji (i < j) the effect of err_i on rating j through
-                // q, q^f of the same bin and the item biases. Forward
-                // substitution then costs one broadcast and one FMA per rating.
-                const bool valid = lane < (int)m;
-                float Mrow[kRound];
-                float pw_d = 1.0f, pwf_d = 1.0f;  // a_i^(j-1-i), a_f^(same-bin ratings between i and j)
+                asm volatile("bar.sync 1, %0;" ::"r"(kCW * 32) : "memory");
+                float wb = 0.0f;
+                if (warp == 0) {
+                    const float sq = (pd[lane] + pd[2 * kRound + lane]) + (pd[4 * kRound + lane] + pd[6 * kRound + lane]);
+                    const float sf =
+                        (pd[kRound + lane] + pd[3 * kRound + lane]) + (pd[5 * kRound + lane] + pd[7 * kRound + lane]);
+                    const float bu_t = myrow[Fs], cu_t = myrow[Fs + 1], res = myrow[Fs + 2];
+                    const uint32_t tb = rec_tbin(keyl);
+                    const bool valid = lane < (int)m;
+                    const float bi0 = st.ib + __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31) +
+                                      __shfl_sync(kFull, fbl < 32 ? st.bf0 : st.bf1, fbl & 31);
+                    float x = ((gb + bu_t + bi0 * cu_t) + (V[lane] * sq + V[kRound + lane] * sf)) - res;
+                    x = valid ? x : 0.0f;
+                    // Forward substitution in blocks of four: each block's
+                    // four values are broadcast at once, every lane solves
+                    // the block's 4x4 system, and the lanes past the block
+                    // subtract its contributions. M is zero on and above the
+                    // diagonal, so the lanes of the block get their own value
+                    // and earlier lanes keep theirs.
+                    const float* Mr = Mb + (size_t)lane * kMS;
 #pragma unroll
-                for (int i = kRound - 1; i >= 0; --i) {
-                    const float gij = gm[i * kGramStride + lane];
-                    const float cui = __shfl_sync(kFull, cu_t, i);
-                    const uint32_t ti = __shfl_sync(kFull, tb, i), fi = __shfl_sync(kFull, fb, i);
-                    const bool before = i < lane, same_f = fi == fb, same_t = ti == tb;
-                    const float bias_lr = p.lr_ib + (same_t ? p.lr_ti : 0.0f) + (same_f ? p.lr_ibf : 0.0f);
-                    const float v = cu_t * cui * bias_lr + p.lr_i * pw_d * gij + (same_f ? p.lr_iqf * pwf_d * gij : 0.0f);
-                    Mrow[i] = before ? v : 0.0f;
-                    if (before) {
-                        pw_d *= a_i;
-                        if (same_f) pwf_d *= a_f;
+                    for (int c = 0; c < kRound; c += 4) {
+                        const float s0 = __shfl_sync(kFull, x, c), s1 = __shfl_sync(kFull, x, c + 1);
+                        const float s2 = __shfl_sync(kFull, x, c + 2), s3 = __shfl_sync(kFull, x, c + 3);
+                        const float* B1 = Mb + (size_t)(c + 1) * kMS + c;
+                        const float* B2 = Mb + (size_t)(c + 2) * kMS + c;
+                        const float* B3 = Mb + (size_t)(c + 3) * kMS + c;
+                        const float e1 = fmaf(-B1[0], s0, s1);
+                        const float e2 = fmaf(-B2[1], e1, fmaf(-B2[0], s0, s2));
+                        const float e3 = fmaf(-B3[2], e2, fmaf(-B3[1], e1, fmaf(-B3[0], s0, s3)));
+                        x = fmaf(-Mr[c + 3], e3, fmaf(-Mr[c + 2], e2, fmaf(-Mr[c + 1], e1, fmaf(-Mr[c], s0, x))));
+                    }
+                    const float wq = valid ? p.lr_i * V[2 * kRound + lane] * x : 0.0f;
+                    const float wf = valid ? p.lr_iqf * V[3 * kRound + lane] * x : 0.0f;
+                    const int pv = __float_as_int(V[7 * kRound + lane]);
+                    ap[lane] = make_float4(wq, wf, V[4 * kRound + lane], __uint_as_float(fbl | (uint32_t)(pv + 1) << 8));
+                    wb = valid ? x * cu_t : 0.0f;
+                    sv[2 * kRound + lane] = wb;
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(kCW * 32) : "memory");
+                // q and q^f stripes, kChunk ratings at a time: the chunk's pe
+                // and q^f values are loaded together, a rating whose bin an
+                // earlier rating of the chunk updated takes that value from
+                // registers, and the chunk's rows are stored at its end.
+                const float am = V[6 * kRound];
+#pragma unroll
+                for (int t = 0; t < CPL; ++t) qv[t] *= am;
+#pragma unroll 1
+                for (int c0 = 0; c0 < kRound; c0 += kChunk) {
+                    float pk[kChunk][CPL], ol[kChunk][CPL], nv[kChunk][CPL];
+                    float4 w4[kChunk];
+#pragma unroll
+                    for (int u = 0; u < kChunk; ++u) {
+                        w4[u] = ap[c0 + u];
+                        const uint32_t fk = __float_as_uint(w4[u].w) & 0xffu;
+#pragma unroll
+                        for (int t = 0; t < CPL; ++t) {
+                            const uint32_t sc = warp + kCW * t;
+                            pk[u][t] = sc < NS ? src[(size_t)(c0 + u) * stride + 32 * sc + lane] : 0.0f;
+                            ol[u][t] = sc < NS ? qfs[(size_t)fk * qs + 32 * sc + lane] : 0.0f;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kChunk; ++u) {
+                        const float wq = w4[u].x, wf = w4[u].y, dk = w4[u].z;
+                        const int pv = (int)(__float_as_uint(w4[u].w) >> 8) - 1;
+#pragma unroll
+                        for (int t = 0; t < CPL; ++t) {
+                            qv[t] = fmaf(-wq, pk[u][t], qv[t]);
+                            float o = ol[u][t];
+#pragma unroll
+                            for (int u2 = 0; u2 < u; ++u2) o = pv == c0 + u2 ? nv[u2][t] : o;
+                            nv[u][t] = fmaf(-wf, pk[u][t], dk * o);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kChunk; ++u) {
+                        // (ratings m..31 of a partial round would store stale rows)
+                        if (c0 + u >= (int)m) break;
+                        const uint32_t fk = __float_as_uint(w4[u].w) & 0xffu;
+#pragma unroll
+                        for (int t = 0; t < CPL; ++t) {
+                            const uint32_t sc = warp + kCW * t;
+                            if (sc < NS) qfs[(size_t)fk * qs + 32 * sc + lane] = nv[u][t];
+                        }
                     }
                 }
-                // pw_d = a_i^j, pwf_d = a_f^(earlier ratings of the same bin)
-                const float bi0 = st.ib + __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31) +
-                                  __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
-                float x = ((gb + bu_t + bi0 * cu_t) + (pw_d * sq + pwf_d * sf)) - res;
-                x = valid ? x : 0.0f;
-#pragma unroll
-                for (int i = 0; i < kRound; ++i) x = fmaf(-Mrow[i], __shfl_sync(kFull, x, i), x);
-                const float my_err = x, my_ec = x * cu_t;
-                // weights of the closed-form updates: a_i^(m-1-j), a_f^(later ratings of the same bin), a_i^m
-                float pw = 1.0f, pwf = 1.0f, am = 1.0f;
-#pragma unroll
-                for (int i = 0; i < kRound; ++i) {
-                    const uint32_t fi = __shfl_sync(kFull, fb, i);
-                    const bool inr = i < (int)m, after = inr && i > lane;
-                    am = inr ? am * a_i : am;
-                    pw = after ? pw * a_i : pw;
-                    pwf = (after && fi == fb) ? pwf * a_f : pwf;
-                }
-                const float wq = valid ? p.lr_i * pw * my_err : 0.0f;
-                const float wf = valid ? p.lr_iqf * pwf * my_err : 0.0f;
-                const float wb = valid ? my_ec : 0.0f;
-                // biases
-                st.ib -= p.lr_ib * warp_sum(wb);
-                {
+                if (warp == 0) {
+                    // item biases
+                    st.ib -= p.lr_ib * warp_sum(wb);
                     float dt0 = 0.0f, dt1 = 0.0f, df0 = 0.0f, df1 = 0.0f;
-#pragma unroll 4
-                    for (int k = 0; k < kRound; ++k) {
-                        const float e = __shfl_sync(kFull, wb, k);
-                        const uint32_t tbk = __shfl_sync(kFull, tb, k), fbk = __shfl_sync(kFull, fb, k);
+#pragma unroll 8
+                    for (int c = 0; c < kRound; ++c) {
+                        const float e = sv[2 * kRound + c];
+                        const uint32_t tbk = __float_as_uint(V[8 * kRound + c]), fbk = __float_as_uint(V[5 * kRound + c]);
                         dt0 += lane == (int)tbk ? e : 0.0f;
                         dt1 += lane + 32 == (int)tbk ? e : 0.0f;
                         df0 += lane == (int)fbk ? e : 0.0f;
@@ -685,42 +883,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_item_pass(DeviceState s, EpochP
                     st.bf0 -= p.lr_ibf * df0;
                     st.bf1 -= p.lr_ibf * df1;
                 }
-                // q
-#pragma unroll
-                for (int v = 0; v < VPL; ++v) q[v] *= am;
-#pragma unroll 4
-                for (int k = 0; k < kRound; ++k) {
-                    const float w = __shfl_sync(kFull, wq, k);
-                    float pk[VPL];
-                    row_from_smem<VPL>(src + (size_t)k * stride, lane, pk);
-#pragma unroll
-                    for (int v = 0; v < VPL; ++v) q[v] = fmaf(-w, pk[v], q[v]);
-                }
-                // q^f rows: the first rating of a bin also applies the bin's decay
-                const unsigned same = __match_any_sync(kFull, valid ? fb : 64u + (uint32_t)lane);
-                float dec = 1.0f;
-                if (valid && __ffs(same) - 1 == lane)
-                    for (int z = __popc(same); z > 0; --z) dec *= a_f;
-#pragma unroll 2
-                for (int k = 0; k < kRound; ++k) {
-                    const float w = __shfl_sync(kFull, wf, k), dk = __shfl_sync(kFull, dec, k);
-                    const uint32_t f = __shfl_sync(kFull, fb, k);
-                    float* qrow = qfs + (size_t)f * qs;
-                    float row[VPL], pk[VPL];
-                    row_from_smem<VPL>(qrow, lane, row);
-                    row_from_smem<VPL>(src + (size_t)k * stride, lane, pk);
-#pragma unroll
-                    for (int v = 0; v < VPL; ++v) row[v] = fmaf(-w, pk[v], dk * row[v]);
-#pragma unroll
-                    for (int v = 0; v < VPL; ++v) qrow[Row<VPL>::elem(lane, v)] = row[v];
-                }
-                __syncwarp();
             }
             __syncthreads();
         }
-        if (warp == 0) {
-            Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);
-            store_item_state(s, i, lane, st);
+        if (warp < kCW) {
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const uint32_t sc = warp + kCW * t;
+                if (sc < NS) s.ifeat[(size_t)i * Fs + 32 * sc + lane] = qv[t];
+            }
+            if (warp == 0) store_item_state(s, i, lane, st);
         }
         for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
             __stcg(s.ifeat_freq + (size_t)i * NF * Fs + e, qfs[(e / Fs) * qs + e % Fs]);
@@ -755,21 +927,22 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
         m->launches += 2;
     }
     if (BF) to_bf16(m, s.yfeat, s.n_items, s.Fs, m->m_bf_yfeat.p);
-    launch_rebuild_ycache(m);
+    launch_rebuild_ycache(m, s.pyc);
     if (BFU) {
         ProfScope ps(m, "bf16_copies");
-        to_bf16(m, s.ufeat, s.n_users, s.Fs, m->m_bf_ufeat.p);
+        to_bf16(m, s.pyc, s.n_users, s.Fs, m->m_bf_pyc.p);
         to_bf16(m, s.ufeat2, s.n_users, s.Fs, m->m_bf_ufeat2.p);
-        to_bf16(m, s.ycache, s.n_users, s.Fs, m->m_bf_ycache.p);
     }
     {
         ProfScope ps(m, "item_pass");
-        const size_t smem =
-            ((size_t)s.NF * (s.Fs + 4) + s.Fs + 2ull * kRound * (s.Fs + 4) + 2ull * kRound * kGramStride) *
-            sizeof(float);
+        const size_t smem = (size_t)item_smem(s.Fs, s.NF).total * sizeof(float);
         TSVD_CUDA(cudaFuncSetAttribute(k_item_pass<VPL, BFU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        unsigned g = persistent_grid(k_item_pass<VPL, BFU>, smem);
-        k_item_pass<VPL, BFU><<<g, kThreads, smem, m->stream>>>(s, p, bf);
+        int dev = 0, sms = 0, per_sm = 0;
+        TSVD_CUDA(cudaGetDevice(&dev));
+        TSVD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        TSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_item_pass<VPL, BFU>, kItemThreads, smem));
+        const unsigned g = (unsigned)(sms * std::max(per_sm, 1));
+        k_item_pass<VPL, BFU><<<g, kItemThreads, smem, m->stream>>>(s, p, bf);
         TSVD_CUDA(cudaGetLastError());
         m->launches++;
     }
@@ -819,9 +992,8 @@ void stratified_epoch(tsvd_model* m, const EpochParams& p) {
         bf.yfeat = m->m_bf_yfeat.as<__nv_bfloat16>();
     }
     if (prec >= TSVD_PREC_BF16_READ_ALL) {
-        bf.ufeat = m->m_bf_ufeat.as<__nv_bfloat16>();
+        bf.pyc = m->m_bf_pyc.as<__nv_bfloat16>();
         bf.ufeat2 = m->m_bf_ufeat2.as<__nv_bfloat16>();
-        bf.ycache = m->m_bf_ycache.as<__nv_bfloat16>();
     }
     const int vpl = (int)(s.Fs / 32);
     if (prec == TSVD_PREC_FP32) {

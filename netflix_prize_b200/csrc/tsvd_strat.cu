@@ -319,7 +319,7 @@ static_assert(kPW * 4 == kRound, "each producer warp stages four of the round's 
 
 // Shared-memory layout of the item pass, in floats (every offset a multiple of 4).
 struct ItemSmem {
-    uint32_t qfs, qsh, buf, hl, mbuf, vec, pd, sv, ap, pw, total;
+    uint32_t qfs, qsh, buf, hl, mbuf, vec, pd, sv, ap, st, pw, total;
 };
 __host__ __device__ inline ItemSmem item_smem(uint32_t Fs, uint32_t NF) {
     ItemSmem L;
@@ -333,6 +333,7 @@ __host__ __device__ inline ItemSmem item_smem(uint32_t Fs, uint32_t NF) {
     L.pd = o;   o += kCW * 2 * kRound;          // consumers' partial dots
     L.sv = o;   o += 4 * kRound;                // the round's update weights (q, q^f, biases)
     L.ap = o;   o += 4 * kRound;                // per rating {w_q, w_f, decay, bin | previous << 8}
+    L.st = o;   o += 132;                       // the item's biases: ib, bit_bin[64], ibias_freq[64]
     L.pw = o;   o += 2 * 36;                    // a_i^n, a_f^n for n = 0..kRound
     L.total = o;
     return L;
@@ -522,7 +523,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
     constexpr int CPL = (VPL + kCW - 1) / kCW;  // 32-column stripes per consumer warp
     constexpr int kChunk = 8;                   // ratings per step of the consumers' apply
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t Fs = s.Fs, NF = s.NF, NS = Fs / 32;
+    const uint32_t Fs = s.Fs, NF = s.NF, T = s.T, NS = Fs / 32;
     const uint32_t stride = Fs + 4;  // one staged rating: pe row + {bu_t, cu_t, res, key}
     const uint32_t qs = Fs + 4;      // padded q^f row stride
     const ItemSmem L = item_smem(Fs, NF);
@@ -536,6 +537,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
     float* pd = smem + L.pd;
     float* sv = smem + L.sv;
     float4* ap = reinterpret_cast<float4*>(smem + L.ap);
+    float* sst = smem + L.st;
     float* apow = smem + L.pw;  // apow[n] = a_i^n, fpow[n] = a_f^n (products in order)
     float* fpow = apow + 36;
     // update factors: x - lr (g + reg x) = a x - lr g
@@ -574,32 +576,59 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
             qfs[(e / Fs) * qs + e % Fs] = __ldcg(s.ifeat_freq + (size_t)i * NF * Fs + e);
         const uint64_t n = b - a;
         const uint32_t rounds = (uint32_t)((n + kRound - 1) / kRound);
+        if (threadIdx.x < 64) {
+            const uint32_t t = threadIdx.x;
+            if (t == 0) sst[0] = __ldcg(s.ibias + i);
+            sst[1 + t] = t < T ? __ldcg(s.bit_bin + (size_t)i * T + t) : 0.0f;
+            sst[65 + t] = t < NF ? __ldcg(s.ibias_freq + (size_t)i * NF + t) : 0.0f;
+        }
         float qv[CPL];  // consumer warp c: q columns 32 (c + kCW t) + lane
-        ItemState st{};
         if (warp < kCW) {
 #pragma unroll
             for (int t = 0; t < CPL; ++t) {
                 const uint32_t sc = warp + kCW * t;
                 qv[t] = sc < NS ? __ldcg(s.ifeat + (size_t)i * Fs + 32 * sc + lane) : 0.0f;
             }
-            if (warp == 0) st = load_item_state(s, i, lane);
         }
         auto round_len = [&](uint32_t r) -> uint32_t {
             const uint64_t left = n - (uint64_t)r * kRound;
             return (uint32_t)(left < (uint64_t)kRound ? left : (uint64_t)kRound);
         };
-        // Producers hold the next round's records (one per lane) and, on the
-        // lanes whose rows they stage, its user-side scalars, loaded a round
-        // ahead so that their latency overlaps the wait for the consumers.
-        Rec nx{};
-        float nbu = 0.0f, ncu = 0.0f;
-        auto prefetch = [&](uint32_t r) {
+        // Producers load records two rounds ahead (one per lane) and the next
+        // round's user scalars (on the lanes that stage them) a round ahead,
+        // so that their latency overlaps the wait for the consumers.
+        Rec rc1{}, rc2{};
+        float us[7] = {};  // ubias, but_bin, alpha_u, ubias_day, ycache_bias, cu, cut
+        // user rows (p_u + ycache_u, p2_u) of ratings pw and pw + 8 of the next
+        // round, loaded at the end of the previous producer phase
+        float px0[VPL], py0[VPL], px1[VPL], py1[VPL];
+        auto fetch_rows0 = [&](uint32_t r) {  // rc1 holds round r's records
             const int pw = warp - kCW;
-            const bool valid = lane < (int)round_len(r);
-            nx = Rec{};
-            nbu = ncu = 0.0f;
-            if (valid) nx = load_rec(s.irec + a + (uint64_t)r * kRound + lane);
-            if (valid && (lane & (kPW - 1)) == pw) user_scalars(s, nx, nbu, ncu);
+            const uint32_t m = round_len(r), j0 = pw, j1 = pw + kPW;
+            const uint32_t u0 = rec_id(__shfl_sync(kFull, rc1.key, j0));
+            const uint32_t u1 = rec_id(__shfl_sync(kFull, rc1.key, j1));
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) px0[v] = py0[v] = px1[v] = py1[v] = 0.0f;
+            if (j0 < m) pe_rows<VPL, BF>(s, bf, u0, lane, px0, py0);
+            if (j1 < m) pe_rows<VPL, BF>(s, bf, u1, lane, px1, py1);
+        };
+        auto fetch_records = [&](uint32_t r, Rec& out) {
+            out = Rec{};
+            if (r < rounds && lane < (int)round_len(r)) out = load_rec(s.irec + a + (uint64_t)r * kRound + lane);
+        };
+        auto fetch_scalars = [&](uint32_t r) {  // rc1 holds round r's records
+            const int pw = warp - kCW;
+            if (lane < (int)round_len(r) && (lane & (kPW - 1)) == pw) {
+                const uint32_t u = rec_id(rc1.key), tb = rec_tbin(rc1.key);
+                const bool hud = rc1.ud < s.n_ud;
+                us[0] = __ldg(s.ubias + u);
+                us[1] = __ldg(s.but_bin + (size_t)u * s.T + tb);
+                us[2] = __ldg(s.alpha_u + u);
+                us[3] = hud ? __ldg(s.ubias_day + rc1.ud) : 0.0f;
+                us[4] = __ldg(s.ycache_bias + u);
+                us[5] = __ldg(s.cu + u);
+                us[6] = hud ? __ldg(s.cut + rc1.ud) : 0.0f;
+            }
         };
         // Producer warp pw: round r's pe rows pw, pw + 8, pw + 16, pw + 24 and
         // their scalars, then (pw < 6) a Gram tile and the entries of the
@@ -611,33 +640,46 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
             float* V = vec + (size_t)(r & 1) * kVecs * kRound;
             const uint32_t m = round_len(r);
             const bool valid = lane < (int)m;
-            const Rec mine = nx;
+            const Rec mine = rc1;
             if ((lane & (kPW - 1)) == pw) {
+                // bu_t, cu_t as user_scalars forms them (src/tsvdx4p.rs:690-708)
+                const float bu = valid ? us[0] + us[1] + us[2] * mine.dev + us[3] + us[4] : 0.0f;
+                const float cu = valid ? us[5] + us[6] : 0.0f;
                 float* row = dst + (size_t)lane * stride;
-                row[Fs] = nbu;
-                row[Fs + 1] = ncu;
+                row[Fs] = bu;
+                row[Fs + 1] = cu;
                 row[Fs + 2] = mine.res;
                 row[Fs + 3] = __uint_as_float(mine.key);
             }
-            // two ratings' user rows in flight; rows m..31 of a partial round are zero
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                const uint32_t j0 = pw + 16 * h, j1 = j0 + kPW;
-                const uint32_t u0 = rec_id(__shfl_sync(kFull, mine.key, j0));
-                const uint32_t u1 = rec_id(__shfl_sync(kFull, mine.key, j1));
-                const float d0 = __shfl_sync(kFull, mine.dev, j0), d1 = __shfl_sync(kFull, mine.dev, j1);
-                float x0[VPL], y0[VPL], x1[VPL], y1[VPL];
+            // ratings pw + 16 and pw + 24: their user rows are loaded now, while
+            // ratings pw and pw + 8 (loaded a phase earlier) are staged; rows
+            // m..31 of a partial round are zero
+            {
+                const uint32_t j2 = pw + 16, j3 = pw + 24;
+                const uint32_t u2 = rec_id(__shfl_sync(kFull, mine.key, j2));
+                const uint32_t u3 = rec_id(__shfl_sync(kFull, mine.key, j3));
+                float x2[VPL], y2[VPL], x3[VPL], y3[VPL];
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) x0[v] = y0[v] = x1[v] = y1[v] = 0.0f;
-                if (j0 < m) pe_rows<VPL, BF>(s, bf, u0, lane, x0, y0);
-                if (j1 < m) pe_rows<VPL, BF>(s, bf, u1, lane, x1, y1);
+                for (int v = 0; v < VPL; ++v) x2[v] = y2[v] = x3[v] = y3[v] = 0.0f;
+                if (j2 < m) pe_rows<VPL, BF>(s, bf, u2, lane, x2, y2);
+                if (j3 < m) pe_rows<VPL, BF>(s, bf, u3, lane, x3, y3);
+                const uint32_t j0 = pw, j1 = pw + kPW;
+                const float d0 = __shfl_sync(kFull, mine.dev, j0), d1 = __shfl_sync(kFull, mine.dev, j1);
+                const float d2 = __shfl_sync(kFull, mine.dev, j2), d3 = __shfl_sync(kFull, mine.dev, j3);
 #pragma unroll
                 for (int v = 0; v < VPL; ++v) {
-                    x0[v] = x0[v] + d0 * y0[v];
-                    x1[v] = x1[v] + d1 * y1[v];
+                    px0[v] = px0[v] + d0 * py0[v];
+                    px1[v] = px1[v] + d1 * py1[v];
                 }
-                stage_row<VPL>(dst + (size_t)j0 * stride, hl + (size_t)j0 * hp, hl + (size_t)(kRound + j0) * hp, lane, x0);
-                stage_row<VPL>(dst + (size_t)j1 * stride, hl + (size_t)j1 * hp, hl + (size_t)(kRound + j1) * hp, lane, x1);
+                stage_row<VPL>(dst + (size_t)j0 * stride, hl + (size_t)j0 * hp, hl + (size_t)(kRound + j0) * hp, lane, px0);
+                stage_row<VPL>(dst + (size_t)j1 * stride, hl + (size_t)j1 * hp, hl + (size_t)(kRound + j1) * hp, lane, px1);
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) {
+                    x2[v] = x2[v] + d2 * y2[v];
+                    x3[v] = x3[v] + d3 * y3[v];
+                }
+                stage_row<VPL>(dst + (size_t)j2 * stride, hl + (size_t)j2 * hp, hl + (size_t)(kRound + j2) * hp, lane, x2);
+                stage_row<VPL>(dst + (size_t)j3 * stride, hl + (size_t)j3 * hp, hl + (size_t)(kRound + j3) * hp, lane, x3);
             }
             // all rows of the round are in place before the Gram products
             asm volatile("bar.sync 2, %0;" ::"r"(kPW * 32) : "memory");
@@ -719,10 +761,19 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                 V[7 * kRound + lane] = __int_as_float(earlier ? 31 - __clz((int)earlier) : -1);
                 V[8 * kRound + lane] = __uint_as_float(rec_tbin(mine.key));
             }
-            if (r + 1 < rounds) prefetch(r + 1);
+            // the next rounds' loads
+            rc1 = rc2;
+            if (r + 1 < rounds) {
+                fetch_scalars(r + 1);
+                fetch_rows0(r + 1);
+            }
+            fetch_records(r + 2, rc2);
         };
         if (warp >= kCW) {
-            prefetch(0);
+            fetch_records(0, rc1);
+            fetch_records(1, rc2);
+            fetch_scalars(0);
+            fetch_rows0(0);
             produce(0);
         }
         __syncthreads();
@@ -787,8 +838,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                     const float bu_t = myrow[Fs], cu_t = myrow[Fs + 1], res = myrow[Fs + 2];
                     const uint32_t tb = rec_tbin(keyl);
                     const bool valid = lane < (int)m;
-                    const float bi0 = st.ib + __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31) +
-                                      __shfl_sync(kFull, fbl < 32 ? st.bf0 : st.bf1, fbl & 31);
+                    const float bi0 = sst[0] + sst[1 + tb] + sst[65 + fbl];
                     float x = ((gb + bu_t + bi0 * cu_t) + (V[lane] * sq + V[kRound + lane] * sf)) - res;
                     x = valid ? x : 0.0f;
                     // Forward substitution in blocks of four: each block's
@@ -865,23 +915,26 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                         }
                     }
                 }
-                if (warp == 0) {
-                    // item biases
-                    st.ib -= p.lr_ib * warp_sum(wb);
-                    float dt0 = 0.0f, dt1 = 0.0f, df0 = 0.0f, df1 = 0.0f;
+                if (warp < 2) {
+                    // item biases: warp 0 the item bias and the time-bin
+                    // biases, warp 1 the frequency-bin biases
+                    if (warp == 0) {
+                        const float sw = warp_sum(wb);
+                        if (lane == 0) sst[0] = sst[0] - p.lr_ib * sw;
+                    }
+                    const int vo = warp == 0 ? 8 : 5;  // the ratings' bins: tb (vector 8) or fb (vector 5)
+                    float d0 = 0.0f, d1 = 0.0f;
 #pragma unroll 8
                     for (int c = 0; c < kRound; ++c) {
                         const float e = sv[2 * kRound + c];
-                        const uint32_t tbk = __float_as_uint(V[8 * kRound + c]), fbk = __float_as_uint(V[5 * kRound + c]);
-                        dt0 += lane == (int)tbk ? e : 0.0f;
-                        dt1 += lane + 32 == (int)tbk ? e : 0.0f;
-                        df0 += lane == (int)fbk ? e : 0.0f;
-                        df1 += lane + 32 == (int)fbk ? e : 0.0f;
+                        const uint32_t bk = __float_as_uint(V[vo * kRound + c]);
+                        d0 += lane == (int)bk ? e : 0.0f;
+                        d1 += lane + 32 == (int)bk ? e : 0.0f;
                     }
-                    st.bt0 -= p.lr_ti * dt0;
-                    st.bt1 -= p.lr_ti * dt1;
-                    st.bf0 -= p.lr_ibf * df0;
-                    st.bf1 -= p.lr_ibf * df1;
+                    const float lr = warp == 0 ? p.lr_ti : p.lr_ibf;
+                    float* bb = sst + (warp == 0 ? 1 : 65);
+                    bb[lane] = bb[lane] - lr * d0;
+                    bb[lane + 32] = bb[lane + 32] - lr * d1;
                 }
             }
             __syncthreads();
@@ -892,7 +945,12 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                 const uint32_t sc = warp + kCW * t;
                 if (sc < NS) s.ifeat[(size_t)i * Fs + 32 * sc + lane] = qv[t];
             }
-            if (warp == 0) store_item_state(s, i, lane, st);
+        }
+        if (threadIdx.x < 64) {
+            const uint32_t t = threadIdx.x;
+            if (t == 0) s.ibias[i] = sst[0];
+            if (t < T) s.bit_bin[(size_t)i * T + t] = sst[1 + t];
+            if (t < NF) s.ibias_freq[(size_t)i * NF + t] = sst[65 + t];
         }
         for (uint32_t e = threadIdx.x; e < NF * Fs; e += blockDim.x)
             __stcg(s.ifeat_freq + (size_t)i * NF * Fs + e, qfs[(e / Fs) * qs + e % Fs]);

@@ -140,7 +140,11 @@ typedef struct tsvd_gpu_options {
                                 when the whole struct is zero                  */
     int32_t device;          /* CUDA device ordinal                           */
     int32_t warps_per_block; /* 0 = tuned default                             */
-    int32_t reserved[8];
+    int32_t heavy_item_ratings; /* stratified item stratum: items with at least
+                                this many ratings take a whole block (rounds of
+                                32 ratings solved together), the others one
+                                warp each; 0 = default (16384)                 */
+    int32_t reserved[7];
 } tsvd_gpu_options;
 
 typedef struct tsvd_model tsvd_model;

@@ -84,7 +84,8 @@ class TsvdGpuOptions(C.Structure):
         ("nsvd_norm_exp", C.c_float),
         ("device", C.c_int32),
         ("warps_per_block", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("heavy_item_ratings", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 

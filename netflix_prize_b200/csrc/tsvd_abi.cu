@@ -142,6 +142,7 @@ int tsvd_create(const tsvd_config* cfg, const tsvd_gpu_options* opts, const tsvd
         if (m->opts.precision != TSVD_PREC_FP32 && m->opts.schedule != TSVD_SCHED_STRATIFIED)
             throw Error(TSVD_ERR_UNSUPPORTED,
                         "BF16 read copies need the stratified schedule (Hogwild writes the tables it reads)");
+        if (m->opts.heavy_item_ratings < 0) throw Error(TSVD_ERR_INVALID, "heavy_item_ratings must be >= 0");
         int n_dev = 0;
         if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
             throw Error(TSVD_ERR_NO_DEVICE, "no CUDA device is visible");

@@ -123,6 +123,7 @@ struct DeviceState {
     const uint32_t* item_work;  // items in processing order
     uint32_t* counters;         // [8] dynamic work counters
     // fixed-size chunks of the by-item index (deterministic split reductions)
+    uint32_t heavy_min;  // item stratum: items with at least this many ratings take a whole block
     uint32_t n_chunks;
     const uint64_t* chunk_lo;      // [n_chunks + 1] start of each chunk in irec; last = n_train
     const uint32_t* item_chunk0;   // [I+1] first chunk of each item

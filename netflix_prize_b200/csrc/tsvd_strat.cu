@@ -291,8 +291,8 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
 // ---------------------------------------------------------------------------
 // Item stratum. An item's ratings form a serial chain (every update feeds the
 // next dot product), and the most-rated items carry ~0.5% of all ratings
-// each, so the chain of the hottest item bounds the pass. Items with >= kHeavy
-// ratings get a whole CTA of kCW + kPW warps, in rounds of kRound ratings:
+// each, so the chain of the hottest item bounds the pass. Items with at least
+// s.heavy_min ratings (an option, 16384 by default) get a whole CTA of kCW + kPW warps, in rounds of kRound ratings:
 //   producers (kPW warps) gather the next round's user rows into
 //     pe = (p_u + ycache_u) + dev * p2_u plus the rating's bias scalars,
 //     form the round's Gram matrix on the tensor cores and from it the
@@ -305,7 +305,6 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
 // Rounds are double-buffered with one __syncthreads per round. Lighter items
 // take one warp each, with the next rating's rows prefetched into registers.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kHeavy = 1024;
 constexpr int kRound = 32;  // ratings per buffered round
 constexpr uint32_t kMS = kRound + 1;  // padded row stride of the round's system M
 constexpr int kCW = 4;                // consumer warps
@@ -560,7 +559,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
         if (k >= s.n_items) return;
         const uint32_t i = s.item_work[k];
         const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
-        if (b - a < kHeavy) {
+        if (b - a < s.heavy_min) {
             // Items are ordered heaviest first: from here on every item is light.
             if (warp == 0) item_light<VPL, BF>(s, p, bf, i, lane);
             for (;;) {

@@ -34,7 +34,8 @@ class TxModel:
     """A device-resident timeSVD++ model (tsvdx4 / TxModel in tx4 mode)."""
 
     def __init__(self, tr: Dataset, pr, cfg: TxConfig, schedule: int = SCHED_HOGWILD,
-                 precision: int = PREC_FP32, nsvd_norm_exp: float = 1.0, device: int = 0):
+                 precision: int = PREC_FP32, nsvd_norm_exp: float = 1.0, device: int = 0,
+                 heavy_item_ratings: int = 0):
         L = load()
         self._L = L
         self.cfg = cfg
@@ -44,6 +45,7 @@ class TxModel:
         opts.precision = precision
         opts.nsvd_norm_exp = nsvd_norm_exp
         opts.device = device
+        opts.heavy_item_ratings = heavy_item_ratings
         c = cfg.to_c()
         tv = tr.view()
         pv = pr.view() if isinstance(pr, MaskedDataset) else pr.view(masked=True)

@@ -141,17 +141,19 @@ def test_stratified_epoch_matches_oracle_tsvdx4p(small, f):
     assert abs(g.calc_rmse(pr) - o.calc_rmse(pr)) < 1e-5
 
 
-@pytest.mark.parametrize("f", [16, 64, 256])
-def test_stratified_heavy_items_match_oracle_tsvdx4p(f):
-    """Items with thousands of ratings take the item stratum's whole-CTA path,
-    whose serial chain runs 32 ratings per round from Gram-matrix lookahead;
-    it must still follow the reference's per-rating item updates."""
+@pytest.mark.parametrize("f,heavy", [(16, 1024), (64, 1024), (256, 1024), (64, 40)])
+def test_stratified_heavy_items_match_oracle_tsvdx4p(f, heavy):
+    """Items with at least `heavy` ratings take the item stratum's whole-block
+    path, whose serial chain runs 32 ratings per round from Gram-matrix
+    lookahead; it must still follow the reference's per-rating item updates
+    (heavy = 40: nearly every item, most of them ending in a partial round)."""
     from tests.conftest import small_sets
     tr, pr = small_sets(n_users=3000, n_items=80, n_train=90000, seed=13)
     assert np.bincount(tr.item_idxs, minlength=tr.n_items).max() >= 2048
     cfg = lm_cfg(f=f, epochs=2)
     o = po.OracleModel(tr, MaskedDataset(pr), cfg)
-    g = TxModel(tr, MaskedDataset(pr), cfg, schedule=SCHED_STRATIFIED, nsvd_norm_exp=1.0)
+    g = TxModel(tr, MaskedDataset(pr), cfg, schedule=SCHED_STRATIFIED, nsvd_norm_exp=1.0,
+                heavy_item_ratings=heavy)
     for e in (1, 2):
         o.fit_epoch(e, po.SCHED_P, nsvd_norm_exp=1.0, n_threads=1)
         g.fit_epoch(tr, pr, e)

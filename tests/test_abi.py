@@ -62,3 +62,34 @@ def test_null_arguments_are_rejected_without_touching_a_device():
     assert L.tsvd_create(None, None, None, None, C.byref(h)) == 1
     assert L.tsvd_fit_epoch(None, 1) == 1
     assert L.tsvd_predict_batch(None, None, None, None, 0, None) == 1
+
+
+def test_gpu_options_are_validated_before_any_device_call():
+    """Bad options fail at create with TSVD_ERR_INVALID and a message, on a
+    host without a GPU as on one with it."""
+    L = native.load()
+    cfg = TxConfig(n_feat=16).to_c()
+    tv, pv = TsvdDatasetView(), TsvdDatasetView()
+    for field, value, text in (("schedule", 7, "schedule"), ("precision", 9, "precision"),
+                               ("heavy_item_ratings", -1, "heavy_item_ratings")):
+        opts = TsvdGpuOptions()
+        opts.nsvd_norm_exp = 1.0
+        setattr(opts, field, value)
+        h = C.c_void_p()
+        rc = L.tsvd_create(C.byref(cfg), C.byref(opts), C.byref(tv), C.byref(pv), C.byref(h))
+        assert rc == 1, field
+        assert text in L.tsvd_last_global_error().decode()
+        assert not h.value
+
+
+def test_heavy_item_threshold_has_its_header_offset():
+    import subprocess, tempfile
+    code = ('#include "tsvdx4_cuda.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+            'int main(){printf("%zu\\n", offsetof(tsvd_gpu_options, heavy_item_ratings));return 0;}')
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(code)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert int(out[0]) == TsvdGpuOptions.heavy_item_ratings.offset

@@ -182,9 +182,15 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    const int nk = (g.K + TC_K - 1) / TC_K;
-    tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, 0, tsm, tid);
-    tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, 0, tsm + kTcABytes, tid);
+    // split K: block z takes K blocks kb0 .. kb0 + nk - 1 (the host sizes
+    // gridDim.z so that none is empty) and writes its partial tile to slice z
+    const int nk_all = (g.K + TC_K - 1) / TC_K;
+    const int per = (nk_all + (int)gridDim.z - 1) / (int)gridDim.z;
+    const int kb0 = (int)blockIdx.z * per;
+    const int nk = min(nk_all, kb0 + per) - kb0;
+    float* const out_f32 = g.out_f32 ? g.out_f32 + (size_t)blockIdx.z * g.M * g.ldc : nullptr;
+    tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, kb0 * TC_K, tsm, tid);
+    tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, kb0 * TC_K, tsm + kTcABytes, tid);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -218,8 +224,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
                 asm volatile("tcgen05.fence::after_thread_sync;");
             }
             uint8_t* nxt = tsm + (st ^ 1u) * kTcStage;
-            tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, (kb + 1) * TC_K, nxt, tid);
-            tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, (kb + 1) * TC_K, nxt + kTcABytes, tid);
+            tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, (kb0 + kb + 1) * TC_K, nxt, tid);
+            tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, (kb0 + kb + 1) * TC_K, nxt + kTcABytes, tid);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncthreads();
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
                     if (n >= g.N) continue;
                     float x = __uint_as_float(v[j]);
                     if (g.bias) x += g.bias[n];
-                    if (g.out_f32) g.out_f32[(size_t)m * g.ldc + n] = x;
+                    if (out_f32) out_f32[(size_t)m * g.ldc + n] = x;
                     if (g.out_bf16) g.out_bf16[(size_t)m * g.ldc + n] = __float2bfloat16(g.gelu ? gelu_f(x) : x);
                 }
             }
@@ -267,14 +273,41 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TC_N));
 }
 
-// `err` receives 1 when an MMA completion wait ran out (the results are then invalid)
+// Sum of the split-K slices ws[z] (z = 0 .. splits-1, in that order) into out.
+__global__ void k_splitk_sum(const float* __restrict__ ws, int splits, int M, int N, int ldc, float* __restrict__ out) {
+    const size_t total = (size_t)M * N;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t at = (e / N) * ldc + e % N;
+        float acc = ws[at];
+        for (int z = 1; z < splits; ++z) acc += ws[(size_t)z * M * ldc + at];
+        out[at] = acc;
+    }
+}
+
+// `err` receives 1 when an MMA completion wait ran out (the results are then invalid).
+// splits > 1 (FP32 output only, no bias or activation) divides K over that many
+// blocks per tile, through ws (splits * M * ldc floats), summed in a fixed order.
 void gemm(cudaStream_t st, unsigned* err, const __nv_bfloat16* A, int a_km, int lda, const __nv_bfloat16* B, int b_kn, int ldb, int M,
-          int N, int K, const float* bias, float* out_f32, __nv_bfloat16* out_bf16, int ldc, int gelu) {
-    GemmArgs g{A, B, M, N, K, lda, ldb, a_km, b_kn, bias, out_f32, out_bf16, ldc, gelu};
+          int N, int K, const float* bias, float* out_f32, __nv_bfloat16* out_bf16, int ldc, int gelu, int splits = 1,
+          float* ws = nullptr) {
+    const int nk = (K + TC_K - 1) / TC_K;
+    splits = std::max(1, std::min(splits, nk));
+    if (splits > 1) {
+        const int per = (nk + splits - 1) / splits;
+        splits = (nk + per - 1) / per;  // no empty slice
+    }
+    const bool split = splits > 1 && ws && out_f32 && !bias && !out_bf16 && !gelu;
+    if (!split) splits = 1;
+    GemmArgs g{A, B, M, N, K, lda, ldb, a_km, b_kn, bias, split ? ws : out_f32, out_bf16, ldc, gelu};
     TSVD_CUDA(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-    dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M);
+    dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M, splits);
     k_gemm_tc<<<grid, 128, kTcSmem, st>>>(g, err);
     TSVD_CUDA(cudaGetLastError());
+    if (split) {
+        k_splitk_sum<<<(unsigned)std::min<size_t>(((size_t)M * N + 255) / 256, 148 * 8), 256, 0, st>>>(ws, splits, M, N, ldc,
+                                                                                                    out_f32);
+        TSVD_CUDA(cudaGetLastError());
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -541,6 +574,7 @@ struct tsvd_encoder {
     tsvd::DevMem users, h0, h0b, z1, h1b, z2, h2b, y, t, dy, dyb, dh2, dz2b, dh1, dz1b, dh0, part;
     tsvd::DevMem hist, inv_n;  // per batch user: rating and date-bin counts, 1 / history length
     tsvd::DevMem tc_err;       // set by the tensor-core GEMM when an MMA wait ran out
+    tsvd::DevMem ws;           // split-K partial tiles of the weight-gradient GEMMs
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::string err;
@@ -606,7 +640,7 @@ double backward(tsvd_encoder* e, int n) {
     TSVD_CUDA(cudaGetLastError());
     // layer 3
     gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, Op, kHid, O, n, nullptr,
-         P(e, 7).g.as<float>(), nullptr, O, 0);
+         P(e, 7).g.as<float>(), nullptr, O, 0, 8, e->ws.as<float>());
     k_colsum_f<<<(O + 127) / 128, 128, 0, st>>>(e->dy.as<float>(), n, O, P(e, 8).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dyb.as<__nv_bfloat16>(), 0, Op, P(e, 7).wb.as<__nv_bfloat16>(), 0, Op, n, kHid, O, nullptr,
          e->dh2.as<float>(), nullptr, kHid, 0);
@@ -614,7 +648,7 @@ double backward(tsvd_encoder* e, int n) {
                                                            e->dz2b.as<__nv_bfloat16>());
     // layer 2
     gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 1, kHid, e->dz2b.as<__nv_bfloat16>(), 1, kHid, kHid, kHid, n, nullptr,
-         P(e, 5).g.as<float>(), nullptr, kHid, 0);
+         P(e, 5).g.as<float>(), nullptr, kHid, 0, 4, e->ws.as<float>());
     k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz2b.as<__nv_bfloat16>(), n, kHid, P(e, 6).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dz2b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 0, kHid, n, kHid, kHid, nullptr,
          e->dh1.as<float>(), nullptr, kHid, 0);
@@ -622,7 +656,7 @@ double backward(tsvd_encoder* e, int n) {
                                                            e->dz1b.as<__nv_bfloat16>());
     // layer 1
     gemm(st, e->tc_err.as<unsigned>(), e->h0b.as<__nv_bfloat16>(), 1, kEmb, e->dz1b.as<__nv_bfloat16>(), 1, kHid, kEmb, kHid, n, nullptr,
-         P(e, 3).g.as<float>(), nullptr, kHid, 0);
+         P(e, 3).g.as<float>(), nullptr, kHid, 0, 16, e->ws.as<float>());
     k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz1b.as<__nv_bfloat16>(), n, kHid, P(e, 4).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dz1b.as<__nv_bfloat16>(), 0, kHid, P(e, 3).wb.as<__nv_bfloat16>(), 0, kHid, n, kEmb, kHid, nullptr,
          e->dh0.as<float>(), nullptr, kEmb, 0);
@@ -789,6 +823,8 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->hist.alloc((size_t)B * (5 + s.T) * 4);
         e->inv_n.alloc((size_t)B * 4);
         e->tc_err.alloc(4);
+        // split-K slices: dW1 16 x 128 x 512, dW2 4 x 512 x 512, dW3 8 x 512 x O
+        e->ws.alloc(std::max(std::max((size_t)16 * kEmb * kHid, (size_t)4 * kHid * kHid), (size_t)8 * kHid * O) * 4);
         TSVD_CUDA(cudaMemset(e->tc_err.p, 0, 4));
         TSVD_CUDA(cudaDeviceSynchronize());
     });

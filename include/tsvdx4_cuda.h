@@ -143,7 +143,7 @@ typedef struct tsvd_gpu_options {
     int32_t heavy_item_ratings; /* stratified item stratum: items with at least
                                 this many ratings take a whole block (rounds of
                                 32 ratings solved together), the others one
-                                warp each; 0 = default (16384)                 */
+                                warp each; 0 = default (32768)                 */
     int32_t reserved[7];
 } tsvd_gpu_options;
 

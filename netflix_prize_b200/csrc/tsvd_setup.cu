@@ -247,8 +247,8 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     s.T = (uint32_t)c.n_time_bins; s.NF = (uint32_t)c.n_freq_bins;
     // Heavy items run as rounds on a whole block; below the threshold a warp
     // per item is cheaper per rating, as long as its chain stays shorter than
-    // the hottest item's (16384 measured best at the full Netflix shape).
-    s.heavy_min = m->opts.heavy_item_ratings > 0 ? (uint32_t)m->opts.heavy_item_ratings : 16384u;
+    // the hottest item's (32768 measured best at the full Netflix shape).
+    s.heavy_min = m->opts.heavy_item_ratings > 0 ? (uint32_t)m->opts.heavy_item_ratings : 32768u;
     s.n_train = R; s.n_pr = P;
     s.day_range = dr;
     s.gbias = (float)(rsum / (double)R);

@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
 // Item stratum. An item's ratings form a serial chain (every update feeds the
 // next dot product), and the most-rated items carry ~0.5% of all ratings
 // each, so the chain of the hottest item bounds the pass. Items with at least
-// s.heavy_min ratings (an option, 16384 by default) get a whole CTA of kCW + kPW warps, in rounds of kRound ratings:
+// s.heavy_min ratings (an option, 32768 by default) get a whole CTA of kCW + kPW warps, in rounds of kRound ratings:
 //   producers (kPW warps) gather the next round's user rows into
 //     pe = (p_u + ycache_u) + dev * p2_u plus the rating's bias scalars,
 //     form the round's Gram matrix on the tensor cores and from it the
@@ -434,25 +434,39 @@ __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf1
     const float gb = s.gbias;
     for (uint64_t base = a; base < b; base += 32) {
         const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+        // the chunk's records and user-side scalars, one rating per lane
         Rec mine{};
-        if (lane < (int)cnt) mine = load_rec(s.irec + base + lane);
+        float bu_l = 0.0f, cu_l = 0.0f;
+        if (lane < (int)cnt) {
+            mine = load_rec(s.irec + base + lane);
+            user_scalars(s, mine, bu_l, cu_l);
+        }
         float pn[VPL], p2n[VPL];
         pe_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, 0)), lane, pn, p2n);
+        // the q^f row of the current rating's bin; the next rating's row is
+        // loaded a step ahead when its bin differs (this rating leaves it alone)
+        uint32_t fcur = rec_fbin(__shfl_sync(kFull, mine.key, 0));
+        float qfv[VPL];
+        Row<VPL>::load_cg(qf_base + (size_t)fcur * Fs, lane, qfv);
         for (uint32_t j = 0; j < cnt; ++j) {
             const Rec r = shfl_rec(mine, j);
             float pe[VPL];
 #pragma unroll
             for (int v = 0; v < VPL; ++v) pe[v] = pn[v] + r.dev * p2n[v];
             if (j + 1 < cnt) pe_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, j + 1)), lane, pn, p2n);
-            float bu_t, cu_t;
-            user_scalars(s, r, bu_t, cu_t);
-            const uint32_t tb = rec_tbin(r.key), fb = rec_fbin(r.key);
-            float* qrow = qf_base + (size_t)fb * Fs;
-            float qfv[VPL];
-            Row<VPL>::load_cg(qrow, lane, qfv);
+            const float bu_t = __shfl_sync(kFull, bu_l, j), cu_t = __shfl_sync(kFull, cu_l, j);
+            const uint32_t tb = rec_tbin(r.key), fb = fcur;
+            const uint32_t fnext = j + 1 < cnt ? rec_fbin(__shfl_sync(kFull, mine.key, j + 1)) : fcur;
+            float qfn[VPL];
+            if (fnext != fcur) Row<VPL>::load_cg(qf_base + (size_t)fnext * Fs, lane, qfn);
             item_step<VPL>(p, gb, q, [&](int v) -> float& { return qfv[v]; }, pe, bu_t, cu_t, r.res, tb, fb, lane,
                            st);
-            Row<VPL>::store(qrow, lane, qfv);
+            Row<VPL>::store(qf_base + (size_t)fcur * Fs, lane, qfv);
+            if (fnext != fcur) {
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) qfv[v] = qfn[v];
+            }
+            fcur = fnext;
         }
     }
     Row<VPL>::store(s.ifeat + (size_t)i * Fs, lane, q);

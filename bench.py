@@ -14,8 +14,10 @@ preset (src/bin/tsvdx4-new.rs:130-154) and 30 time bins.
            create() (H2D of both sets, setup, seeded init) plus per step
            fit_epoch + calc_rmse on the held-out set (H2D of the pr columns,
            D2H of the result)
-  roofline the user-stratum kernel: algorithmic bytes (28 f + 64 per rating)
-           over its CUDA-event duration, against the measured HBM copy peak
+  roofline the dominant kernel of the measured schedule (stratified: the item
+           stratum, 8 f + 44 algorithmic bytes per rating; Hogwild: the user
+           pass, 28 f + 64) over its CUDA-event duration, against the
+           measured HBM copy peak
 
 --impl reference runs the reference's CPU algorithm (the C++ restatement of
 TxModel in oracle/, since the reference's Rust toolchain is absent) on a
@@ -67,9 +69,10 @@ def B_per_rating(f: int) -> int:
 def kernel_bytes_per_rating(kernel: str, f: int) -> int:
     """Algorithmic bytes per rating of the kernel the roofline is quoted on."""
     if kernel == "item_pass":
-        # item stratum: the rating's user rows p, p2, ycache (12 f), its 16-byte
-        # record and 7 user-side bias scalars; item rows stay on chip per item
-        return 12 * f + 44
+        # item stratum: the rating's two user rows, p_u + ycache_u (summed once
+        # per user by the ycache rebuild) and p2_u (8 f), its 16-byte record and
+        # 7 user-side bias scalars (28 B); item rows stay on chip per item
+        return 8 * f + 44
     return B_per_rating(f)
 
 
@@ -232,36 +235,6 @@ def cpu_baseline(args):
                       f"{args.shape} generator, f={args.f}; host has {os.cpu_count()} cores"}
 
 
-def l2_read_gbs(stream) -> float:
-    """Streaming read bandwidth of an L2-resident buffer (48 MB of FP32, summed
-    50 times by torch on the bench's stream): the on-chip counterpart of the
-    HBM copy peak, for kernels whose working set L2 serves."""
-    import torch
-    x = torch.empty(12 * 1024 * 1024, dtype=torch.float32, device="cuda").uniform_()
-    with torch.cuda.stream(stream):
-        for _ in range(5):
-            x.sum()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(50):
-            x.sum()
-        e1.record(stream)
-    torch.cuda.synchronize()
-    return 50 * x.numel() * 4 / (e0.elapsed_time(e1) / 1000.0) / 1e9
-
-
-def user_pass_l2(kstats, args, R, l2):
-    """The per-user passes against the L2 figure: item-side bytes per rating
-    (Hogwild: q, q^f read + write and y gather + RMW, 28 f; stratified user
-    stratum: q, q^f reads, 8 f) over the pass's duration."""
-    out = {}
-    for kn, bpr in (("user_pass_hogwild", 28 * args.f), ("user_pass_stratified", 8 * args.f)):
-        if kn in kstats:
-            gbs = bpr * R / (kstats[kn]["avg_ms"] / 1000.0) / 1e9
-            out[kn] = {"item_side_bytes_per_rating": bpr, "achieved_gbs": gbs, "frac_of_l2_read": gbs / l2}
-    return out
-
-
 def time_to_rmse(model, tr, pr):
     """Time to a held-out RMSE target for new users (the C5 fold-in): the
     plain form (standard init + user-side SGD passes with item tables frozen)
@@ -386,7 +359,6 @@ def main():
     rmse = model.calc_rmse(pr)
     value = R * args.steps * world / (ms / 1000.0)
     peak, peak_kind = measured_peaks()
-    l2 = l2_read_gbs(stream)
     dom = kstats.get(kname, {"avg_ms": float("nan")})
     bpr = kernel_bytes_per_rating(kname, args.f)
     achieved = bpr * R / (dom["avg_ms"] / 1000.0) / 1e9
@@ -442,9 +414,7 @@ def main():
         "config": workload_config(args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": kname,
-                     "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_rating": bpr,
-                     "l2_read_gbs": l2, "l2_source": "bench: torch sum over a 48 MB L2-resident buffer",
-                     "user_pass_vs_l2": user_pass_l2(kstats, args, R, l2)},
+                     "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_rating": bpr},
         "kernels": kstats,
         "heldout_rmse_after_run": rmse,
         "clocks": clk,

@@ -5,7 +5,7 @@
  * `trait Regressor` (src/lib.rs:616-651), as implemented by `TxModel`
  * (src/tx.rs:457-1116) and driven by `fit2_inner`/`fit` (src/lib.rs:881-996,
  * 764-815). A Rust shim `TxGpuModel: Regressor` binds these symbols one to
- * one; the binding is written out in INTEGRATION.md.
+ * one.
  *
  * Conventions
  *  - Every entry point returns an int status (TSVD_OK == 0). On failure the
@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define TSVD_ABI_VERSION 1
+#define TSVD_ABI_VERSION 2
 
 enum tsvd_status {
     TSVD_OK = 0,
@@ -102,21 +102,26 @@ typedef struct tsvd_dataset_view {
 
 /* Epoch schedules. */
 enum tsvd_schedule {
+    /* Deterministic stratified schedule, the default: the reference's own
+     * parallel schedule (src/tsvdx4p.rs:390-805): a user stratum (users in
+     * parallel, item tables frozen, NSVD1 deltas reduced in a fixed order),
+     * then an item stratum (items in parallel, user tables frozen). Bitwise
+     * reproducible for a given seed; held-out RMSE tracks the sequential
+     * reference within 0.001 per epoch at the full Netflix shape. Covers
+     * both low_memory settings and the ordinal head with lr_t = 0. */
+    TSVD_SCHED_STRATIFIED = 0,
     /* Users in parallel, one warp each, item-side tables updated in place as
      * each rating is processed (the reference's per-rating update order
      * inside a user, src/tx.rs:836-1106); concurrent users race on shared
-     * item rows. Fastest; not bitwise reproducible run to run. */
-    TSVD_SCHED_HOGWILD = 0,
-    /* Deterministic stratified schedule: the reference's own parallel
-     * schedule (src/tsvdx4p.rs:390-805): a user stratum (users in parallel,
-     * item tables frozen, NSVD1 deltas reduced in a fixed order), then an
-     * item stratum (items in parallel, user tables frozen). Bitwise
-     * reproducible for a given seed. */
-    TSVD_SCHED_STRATIFIED = 1,
+     * item rows. Not bitwise reproducible run to run, and unstable at the
+     * full Netflix shape after about 6 epochs of the lm preset (the most
+     * rated items' rows go stale under thousands of concurrent users):
+     * opt-in, for short runs and moderate sizes. n_feat <= 256. */
+    TSVD_SCHED_HOGWILD = 1,
     /* The reference's sequential pass exactly (src/tx.rs:756-1106): one warp
      * takes the users one after another in get_users order, so every rating
-     * sees every earlier update. Slow (one warp on the GPU); for parity runs
-     * and small data. */
+     * sees every earlier update. Slow (one warp on the GPU); for parity runs,
+     * small data, lr_t != 0 and the seq_epochs of the stratified schedule. */
     TSVD_SCHED_SEQUENTIAL = 2
 };
 
@@ -131,20 +136,27 @@ enum tsvd_precision {
                                    ycache_u that the item stratum gathers        */
 };
 
-/* Options that have no counterpart in TxConfig. Zero-initialised = defaults. */
+/* Options that have no counterpart in TxConfig. Passing opts = NULL to
+ * tsvd_create gives the defaults: stratified, FP32, nsvd_norm_exp 1.0,
+ * device 0, no sequential epochs. */
 typedef struct tsvd_gpu_options {
     int32_t schedule;        /* enum tsvd_schedule                            */
     int32_t precision;       /* enum tsvd_precision                           */
     float nsvd_norm_exp;     /* stratified: y-delta divisor exponent
-                                (Tsvdx4pConfig::nsvd_norm_exp), default 1.0
-                                when the whole struct is zero                  */
+                                (Tsvdx4pConfig::nsvd_norm_exp,
+                                src/tsvdx4p.rs:176-179): 0 = sum, 0.5 = sqrt,
+                                1 = mean                                       */
     int32_t device;          /* CUDA device ordinal                           */
     int32_t warps_per_block; /* 0 = tuned default                             */
     int32_t heavy_item_ratings; /* stratified item stratum: items with at least
                                 this many ratings take a whole block (rounds of
                                 32 ratings solved together), the others one
                                 warp each; 0 = default (32768)                 */
-    int32_t reserved[7];
+    int32_t seq_epochs[5];   /* stratified: Tsvdx4pConfig::seq_epochs
+                                (src/tsvdx4p.rs:181-186,815-822): these
+                                1-based epochs run the sequential schedule
+                                instead; 0 = unused slot                       */
+    int32_t reserved[2];
 } tsvd_gpu_options;
 
 typedef struct tsvd_model tsvd_model;
@@ -176,7 +188,10 @@ int tsvd_fit_epoch(tsvd_model* m, uint64_t epoch);
 int tsvd_predict_batch(const tsvd_model* m, const int32_t* u, const int32_t* i,
                        const int16_t* day, uint64_t n, float* out);
 
-/* Same with device pointers, on the model's stream; no host copies. */
+/* Same with device pointers, on the model's stream; no host copies and no
+ * host-side row checks. A row whose user index is outside 0..n_users-1 or
+ * whose item index is outside 0..n_items-1 reads no table and gets a NaN
+ * output. */
 int tsvd_predict_batch_device(const tsvd_model* m, const int32_t* d_u,
                               const int32_t* d_i, const int16_t* d_day,
                               uint64_t n, float* d_out);
@@ -205,6 +220,8 @@ int tsvd_calc_rmse(const tsvd_model* m, const tsvd_dataset_view* ds, double* out
  * Inputs d_u, d_i, d_day, d_target (and d_is_test, which may be NULL) are
  * device arrays of n rows; d_out is a device array of 3 doubles that receives
  * {rmse, sum of squared errors, rows counted} over the is_test == 0 rows.
+ * Rows whose user or item index is out of range are never read; if there is
+ * any, d_out receives {NaN, NaN, -(number of such rows)} instead.
  * The result equals tsvd_calc_rmse's up to FP64 summation order.
  * It calls no allocator: its scratch is a fixed 512 KiB device array inside
  * the library (held by every GPU that loads it until exit), which limits n to

@@ -16,8 +16,8 @@ TSVD_ERR_NO_DEVICE = 4
 TSVD_ERR_OOM = 5
 TSVD_ERR_TIMEOUT = 6
 
-SCHED_HOGWILD = 0
-SCHED_STRATIFIED = 1
+SCHED_STRATIFIED = 0
+SCHED_HOGWILD = 1
 SCHED_SEQUENTIAL = 2
 PREC_FP32 = 0
 PREC_BF16_READ = 1
@@ -85,7 +85,8 @@ class TsvdGpuOptions(C.Structure):
         ("device", C.c_int32),
         ("warps_per_block", C.c_int32),
         ("heavy_item_ratings", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("seq_epochs", C.c_int32 * 5),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

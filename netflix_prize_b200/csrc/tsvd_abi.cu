@@ -7,28 +7,17 @@
 
 using tsvd::Error;
 
+namespace tsvd {
+std::string& global_err() {
+    thread_local std::string e;
+    return e;
+}
+}  // namespace tsvd
+
 namespace {
 
-thread_local std::string g_global_err;
-
-// Runs `f`, mapping exceptions to a status and an error message.
-template <class F>
-int guarded(const tsvd_model* m, F&& f) {
-    try {
-        f();
-        return TSVD_OK;
-    } catch (const Error& e) {
-        if (m) m->err = e.what();
-        g_global_err = e.what();
-        return e.status;
-    } catch (const std::exception& e) {
-        if (m) m->err = e.what();
-        g_global_err = e.what();
-        return TSVD_ERR_INVALID;
-    }
-}
-
-void use_device(const tsvd_model* m) { TSVD_CUDA(cudaSetDevice(m->device)); }
+using tsvd::guarded;
+using tsvd::use_device;
 
 struct ParamRef {
     float* dev;
@@ -117,9 +106,9 @@ extern "C" {
 
 int tsvd_abi_version(void) { return TSVD_ABI_VERSION; }
 
-const char* tsvd_last_global_error(void) { return g_global_err.c_str(); }
+const char* tsvd_last_global_error(void) { return tsvd::global_err().c_str(); }
 
-const char* tsvd_last_error(const tsvd_model* m) { return m ? m->err.c_str() : g_global_err.c_str(); }
+const char* tsvd_last_error(const tsvd_model* m) { return m ? m->err.c_str() : tsvd::global_err().c_str(); }
 
 int tsvd_create(const tsvd_config* cfg, const tsvd_gpu_options* opts, const tsvd_dataset_view* tr,
                 const tsvd_dataset_view* pr, tsvd_model** out) {
@@ -157,7 +146,7 @@ int tsvd_create(const tsvd_config* cfg, const tsvd_gpu_options* opts, const tsvd
         tsvd::setup_model(m, *tr, *pr);
     });
     if (rc != TSVD_OK) {
-        g_global_err = m->err;
+        tsvd::global_err() = m->err;
         tsvd_destroy(m);
         return rc;
     }
@@ -321,6 +310,7 @@ int tsvd_get_param(const tsvd_model* m, const char* name, void* dst, uint64_t nb
         ParamRef r;
         if (!find_param(m, n, r)) throw Error(TSVD_ERR_INVALID, "unknown or unavailable parameter " + n);
         if (nbytes != r.rows * r.cols * 4) throw Error(TSVD_ERR_INVALID, "size mismatch for " + n);
+        if (nbytes == 0) return;  // n_feat = 0: feature tables have no columns
         TSVD_CUDA(cudaMemcpy2DAsync(dst, r.cols * 4, r.dev, r.stride * 4, r.cols * 4, r.rows, cudaMemcpyDeviceToHost,
                                     m->stream));
         TSVD_CUDA(cudaStreamSynchronize(m->stream));
@@ -342,6 +332,7 @@ int tsvd_set_param(tsvd_model* m, const char* name, const void* src, uint64_t nb
         ParamRef r;
         if (!find_param(m, n, r)) throw Error(TSVD_ERR_INVALID, "unknown or unavailable parameter " + n);
         if (nbytes != r.rows * r.cols * 4) throw Error(TSVD_ERR_INVALID, "size mismatch for " + n);
+        if (nbytes == 0) return;
         TSVD_CUDA(cudaMemcpy2DAsync(r.dev, r.stride * 4, src, r.cols * 4, r.cols * 4, r.rows, cudaMemcpyHostToDevice,
                                     m->stream));
         TSVD_CUDA(cudaStreamSynchronize(m->stream));

@@ -312,6 +312,158 @@ __global__ void __launch_bounds__(kThreads) k_rebuild_ycache_day(DeviceState s) 
     }
 }
 
+// The sequential pass for n_feat > 256 (low_memory, no ordinal head): one
+// warp, users in get_users order; the user's rows and the rated item's rows
+// are read and written in 256-column slices, in two passes per rating (the
+// dot product, then the updates), with the user's NSVD1 error sum kept in the
+// user's g_user row. Per element the arithmetic is seq_user's.
+constexpr int kWV = 8;
+constexpr uint32_t kSlice = 32 * kWV;
+
+__global__ void __launch_bounds__(32) k_seq_wide(DeviceState s, EpochParams p, const uint32_t* __restrict__ order,
+                                                 uint32_t n_work) {
+    using R8 = Row<kWV>;
+    const int lane = threadIdx.x & 31;
+    const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
+    const float gb = s.gbias;
+    for (uint32_t k = 0; k < n_work; ++k) {
+        const uint32_t u = order[k];
+        const uint64_t start = s.user_off[u], end = s.user_off[u + 1];
+        if (start == end) continue;
+        const uint64_t n = end - start;
+        const Rec* rr = s.rec + start;
+        const uint64_t ps = s.pr_off[u], pe_ = s.pr_off[u + 1];
+        const uint64_t total = n + (p.full_su ? (pe_ - ps) : 0);
+        const float norm = sqrtf((float)total);
+        float* pu_row = s.ufeat + (size_t)u * Fs;
+        float* p2_row = s.ufeat2 + (size_t)u * Fs;
+        float* su_row = s.ycache + (size_t)u * Fs;
+        float* sq_row = s.g_user + (size_t)u * Fs;
+        // su (src/tx.rs:800-822) from the current y, slice by slice
+        float sub = 0.0f;
+        for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+            float su[kWV], sb = 0.0f;
+#pragma unroll
+            for (int v = 0; v < kWV; ++v) su[v] = 0.0f;
+            gather_rows8<kWV>(s.yfeat + c0, c0 == 0 ? s.ybias : nullptr, Fs, n,
+                              [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sb);
+            if (p.full_su) {
+                const uint32_t* pp = s.pr_item + ps;
+                gather_rows8<kWV>(s.yfeat + c0, c0 == 0 ? s.ybias : nullptr, Fs, pe_ - ps,
+                                  [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sb);
+            }
+#pragma unroll
+            for (int v = 0; v < kWV; ++v) su[v] = su[v] / norm;
+            R8::store(su_row + c0, lane, su);
+            const float z[kWV] = {};
+            R8::store(sq_row + c0, lane, z);
+            if (c0 == 0) sub = sb / norm;
+        }
+        if (lane == 0) s.ycache_bias[u] = sub;
+        float ub = __ldcg(s.ubias + u), al = __ldcg(s.alpha_u + u), cuu = __ldcg(s.cu + u);
+        float sum_err = 0.0f;
+        for (uint64_t t = 0; t < n; ++t) {
+            const Rec r = load_rec(rr + t);
+            const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+            const uint32_t ud = r.ud;
+            const bool hud = ud < s.n_ud;
+            const float dv = r.dev;
+            float sc[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            if (lane == 0) {
+                sc[0] = __ldcg(s.ibias + i);
+                sc[1] = __ldcg(s.bit_bin + (size_t)i * T + tb);
+                sc[2] = __ldcg(s.ibias_freq + (size_t)i * NF);  // low_memory trains bin 0
+                sc[3] = hud ? __ldcg(s.cut + ud) : 0.0f;
+                sc[4] = hud ? __ldcg(s.ubias_day + ud) : 0.0f;
+                sc[5] = __ldcg(s.but_bin + (size_t)u * T + tb);
+            }
+#pragma unroll
+            for (int c = 0; c < 6; ++c) sc[c] = __shfl_sync(kFull, sc[c], 0);
+            const float ib = sc[0], bit = sc[1], ibf = sc[2], ct = sc[3], bud = sc[4], but = sc[5];
+            const float bu_t = ub + but + al * dv + bud + sub;
+            const float bi_t = ib + bit + ibf;
+            const float cu_t = cuu + ct;
+            float* q_row = s.ifeat + (size_t)i * Fs;
+            float* qf_row = s.ifeat_freq + (size_t)i * NF * Fs;
+            float part = 0.0f;
+            for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                float q[kWV], qf[kWV], pu[kWV], su[kWV], p2[kWV];
+                R8::load_cg(q_row + c0, lane, q);
+                R8::load_cg(qf_row + c0, lane, qf);
+                R8::load_cg(pu_row + c0, lane, pu);
+                R8::load_cg(su_row + c0, lane, su);
+                R8::load_cg(p2_row + c0, lane, p2);
+#pragma unroll
+                for (int v = 0; v < kWV; ++v) part += ((pu[v] + su[v]) + dv * p2[v]) * (q[v] + qf[v]);
+            }
+            const float dot = warp_sum(part);
+            const float err = (gb + bu_t + bi_t * cu_t + dot) - r.res;
+            const float err_b = err * p.w_bias, err_d = err * p.w_factor;
+            // bias updates (src/tx.rs:978-987)
+            ub -= p.lr_ub * err_b;
+            al -= p.lr_ta * err_b * dv;
+            if (lane == 0) {
+                s.but_bin[(size_t)u * T + tb] = but - p.lr_tu * err_b;
+                if (hud) s.ubias_day[ud] = bud - p.lr_ubd * err_b;
+                s.ibias[i] = ib - p.lr_ib * (err_b * cu_t);
+                s.bit_bin[(size_t)i * T + tb] = bit - p.lr_ti * (err_b * cu_t);
+                s.ibias_freq[(size_t)i * NF] = ibf - p.lr_ibf * (err_b * cu_t);
+            }
+            cuu -= p.lr_cu * (err_b * bi_t + p.reg_cu * (cuu - 1.0f));
+            // factor updates (src/tx.rs:992-1023)
+            if (!p.sum_err_bug) sum_err += err_b;
+            else
+                for (uint32_t kk = 0; kk < s.F; ++kk) sum_err += err_b;
+            for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                float q[kWV], qf[kWV], pu[kWV], su[kWV], p2[kWV], sq[kWV];
+                R8::load_cg(q_row + c0, lane, q);
+                R8::load_cg(qf_row + c0, lane, qf);
+                R8::load_cg(pu_row + c0, lane, pu);
+                R8::load_cg(su_row + c0, lane, su);
+                R8::load_cg(p2_row + c0, lane, p2);
+                R8::load_cg(sq_row + c0, lane, sq);
+#pragma unroll
+                for (int v = 0; v < kWV; ++v) {
+                    const float qe = q[v] + qf[v];
+                    const float pk = pu[v], p2k = p2[v];
+                    sq[v] += err_d * qe;
+                    pu[v] = pk - p.lr_u * (err_d * qe + p.reg_u * pk);
+                    p2[v] = p2k - p.lr_u2 * (err_d * qe * dv + p.reg_u2 * p2k);
+                    const float pe = pk + dv * p2k + 0.0f + su[v];
+                    q[v] = q[v] + -(p.lr_i * (err_d * pe + p.reg_i * q[v]));
+                    qf[v] = qf[v] + -(p.lr_iqf * (err_d * pe + p.reg_iqf * qf[v]));
+                }
+                R8::store(pu_row + c0, lane, pu);
+                R8::store(p2_row + c0, lane, p2);
+                R8::store(sq_row + c0, lane, sq);
+                R8::store(q_row + c0, lane, q);
+                R8::store(qf_row + c0, lane, qf);
+            }
+            __syncwarp();  // lane 0's scalar writes before the next rating's reads
+        }
+        if (lane == 0) {
+            s.ubias[u] = ub;
+            s.alpha_u[u] = al;
+            s.cu[u] = cuu;
+        }
+        // NSVD1 factor & bias updates at the end of the user (src/tx.rs:1099-1106)
+        const float eb = sum_err / norm;
+        for (uint64_t t = 0; t < n; ++t) {
+            const uint32_t j = rec_id(__ldg(&rr[t].key));
+            for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                float g[kWV], y[kWV];
+                R8::load_cg(sq_row + c0, lane, g);
+                R8::load_cg(s.yfeat + (size_t)j * Fs + c0, lane, y);
+#pragma unroll
+                for (int v = 0; v < kWV; ++v) y[v] = y[v] + -(p.lr_y * (g[v] / norm + p.reg_y * y[v]));
+                R8::store(s.yfeat + (size_t)j * Fs + c0, lane, y);
+            }
+            if (lane == 0) s.ybias[j] = s.ybias[j] + -(p.lr_yb * eb);
+            __syncwarp();
+        }
+    }
+}
+
 template <int VPL, bool DAY>
 void launch_seq(tsvd_model* m, const EpochParams& p, const uint32_t* order, bool sequential) {
     const unsigned g = sequential ? 1u : persistent_grid(k_seq_pass<VPL, DAY>, 0);
@@ -335,7 +487,13 @@ void day_epoch_pass(tsvd_model* m, const uint32_t* order, bool sequential) {
     const EpochParams p = make_params(m);
     const int vpl = (int)(m->d.Fs / 32);
     ProfScope ps(m, sequential ? "user_pass_sequential" : "user_pass_hogwild_day");
-    if (m->cfg.low_memory) {
+    if (m->d.Fs > kSlice) {
+        // n_feat > 256: sequential only (create() rejects Hogwild there)
+        if (!sequential) throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256 needs the stratified or sequential schedule");
+        k_seq_wide<<<1, 32, 0, m->stream>>>(m->d, p, order, m->d.n_users);
+        TSVD_CUDA(cudaGetLastError());
+        m->launches++;
+    } else if (m->cfg.low_memory) {
         TSVD_DISPATCH(vpl, (launch_seq<V, false>(m, p, order, sequential)));
     } else {
         TSVD_DISPATCH(vpl, (launch_seq<V, true>(m, p, order, sequential)));

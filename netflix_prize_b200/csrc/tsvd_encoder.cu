@@ -290,6 +290,8 @@ __global__ void k_splitk_sum(const float* __restrict__ ws, int splits, int M, in
 void gemm(cudaStream_t st, unsigned* err, const __nv_bfloat16* A, int a_km, int lda, const __nv_bfloat16* B, int b_kn, int ldb, int M,
           int N, int K, const float* bias, float* out_f32, __nv_bfloat16* out_bf16, int ldc, int gelu, int splits = 1,
           float* ws = nullptr) {
+    // K = 0 would issue no MMA and leave the accumulator uninitialised
+    if (M <= 0 || N <= 0 || K <= 0) throw Error(TSVD_ERR_INVALID, "gemm: M, N and K must be positive");
     const int nk = (K + TC_K - 1) / TC_K;
     splits = std::max(1, std::min(splits, nk));
     if (splits > 1) {
@@ -715,6 +717,7 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->lr = lr;
         e->wd = weight_decay;
         const DeviceState& s = m->d;
+        if (s.F < 1 || s.F > 256) throw Error(TSVD_ERR_UNSUPPORTED, "the user encoder is built for n_feat in 1..256");
         e->O = (int)s.F + 2;
         e->Op = (e->O + 7) & ~7;
         TSVD_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));

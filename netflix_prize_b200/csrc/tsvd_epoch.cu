@@ -367,7 +367,60 @@ __global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, cons
 
 template <int VPL>
 __device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bfloat16* __restrict__ ybf, uint32_t u,
-                                             int lane, float* __restrict__ pyc);
+                                             int lane, float* __restrict__ pyc) {
+    constexpr int B = 8;  // rows in flight
+    const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
+    const uint64_t pa = s.pr_off[u], pb = s.pr_off[u + 1];
+    const uint64_t ntr = b - a, n = ntr + (pb - pa);
+    const int32_t cnt_all = s.user_cnt_tr[u] + s.user_cnt_pr[u];
+    // rows wider than 32 * VPL columns (n_feat > 256) in slices of 32 * VPL
+    for (uint32_t c0 = 0; c0 < s.Fs; c0 += 32 * VPL) {
+        float su[VPL];
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
+        float sub = 0.0f;
+        for (uint64_t base = 0; base < n; base += 32) {
+            const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
+            const uint64_t q = base + lane;
+            uint32_t mine = 0;
+            if (lane < (int)cnt) mine = q < ntr ? rec_id(__ldg(&s.rec[a + q].key)) : __ldg(s.pr_item + pa + (q - ntr));
+            for (uint32_t j = 0; j < cnt; j += B) {
+                float y[B][VPL], yb[B];
+#pragma unroll
+                for (int t = 0; t < B; ++t) {
+                    const uint32_t it = __shfl_sync(kFull, mine, j + t < cnt ? j + t : cnt - 1);
+                    if (ybf) row_load_bf16<VPL>(ybf + (size_t)it * s.Fs + c0, lane, y[t]);
+                    else Row<VPL>::load_nc(s.yfeat + (size_t)it * s.Fs + c0, lane, y[t]);
+                    yb[t] = c0 == 0 ? __ldg(s.ybias + it) : 0.0f;
+                }
+#pragma unroll
+                for (int t = 0; t < B; ++t) {
+                    if (j + t < cnt) {
+#pragma unroll
+                        for (int v = 0; v < VPL; ++v) su[v] += y[t][v];
+                        sub += yb[t];
+                    }
+                }
+            }
+        }
+        if (cnt_all > 0) {
+            const float nrm = sqrtf((float)cnt_all);
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) su[v] = su[v] / nrm;
+            sub = sub / nrm;
+        }
+        Row<VPL>::store(s.ycache + (size_t)u * s.Fs + c0, lane, su);
+        if (lane == 0 && c0 == 0) s.ycache_bias[u] = sub;
+        if (pyc) {
+            // p_u + ycache_u, the user-side sum every item-stratum rating of u reads
+            float pu[VPL];
+            Row<VPL>::load_cg(s.ufeat + (size_t)u * s.Fs + c0, lane, pu);
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) pu[v] = pu[v] + su[v];
+            Row<VPL>::store(pyc + (size_t)u * s.Fs + c0, lane, pu);
+        }
+    }
+}
 
 // Batched ycache rebuild over (variant, user) pairs, variant-major.
 __global__ void __launch_bounds__(kThreads) k_rebuild_batched(const DeviceState* __restrict__ states,
@@ -398,62 +451,6 @@ __global__ void __launch_bounds__(kThreads) k_rebuild_ycache(DeviceState s, cons
     const uint32_t warps = gridDim.x * kWarps;
     for (uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5); u < s.n_users; u += warps)
         rebuild_user<VPL>(s, ybf, u, lane, pyc);
-}
-
-template <int VPL>
-__device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bfloat16* __restrict__ ybf, uint32_t u,
-                                             int lane, float* __restrict__ pyc) {
-    constexpr int B = 8;  // rows in flight
-    {
-        float su[VPL];
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
-        float sub = 0.0f;
-        const uint64_t a = s.user_off[u], b = s.user_off[u + 1];
-        const uint64_t pa = s.pr_off[u], pb = s.pr_off[u + 1];
-        const uint64_t ntr = b - a, n = ntr + (pb - pa);
-        for (uint64_t base = 0; base < n; base += 32) {
-            const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
-            const uint64_t q = base + lane;
-            uint32_t mine = 0;
-            if (lane < (int)cnt) mine = q < ntr ? rec_id(__ldg(&s.rec[a + q].key)) : __ldg(s.pr_item + pa + (q - ntr));
-            for (uint32_t j = 0; j < cnt; j += B) {
-                float y[B][VPL], yb[B];
-#pragma unroll
-                for (int t = 0; t < B; ++t) {
-                    const uint32_t it = __shfl_sync(kFull, mine, j + t < cnt ? j + t : cnt - 1);
-                    if (ybf) row_load_bf16<VPL>(ybf + (size_t)it * s.Fs, lane, y[t]);
-                    else Row<VPL>::load_nc(s.yfeat + (size_t)it * s.Fs, lane, y[t]);
-                    yb[t] = __ldg(s.ybias + it);
-                }
-#pragma unroll
-                for (int t = 0; t < B; ++t) {
-                    if (j + t < cnt) {
-#pragma unroll
-                        for (int v = 0; v < VPL; ++v) su[v] += y[t][v];
-                        sub += yb[t];
-                    }
-                }
-            }
-        }
-        const int32_t cnt = s.user_cnt_tr[u] + s.user_cnt_pr[u];
-        if (cnt > 0) {
-            const float nrm = sqrtf((float)cnt);
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) su[v] = su[v] / nrm;
-            sub = sub / nrm;
-        }
-        Row<VPL>::store(s.ycache + (size_t)u * s.Fs, lane, su);
-        if (lane == 0) s.ycache_bias[u] = sub;
-        if (pyc) {
-            // p_u + ycache_u, the user-side sum every item-stratum rating of u reads
-            float pu[VPL];
-            Row<VPL>::load_cg(s.ufeat + (size_t)u * s.Fs, lane, pu);
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) pu[v] = pu[v] + su[v];
-            Row<VPL>::store(pyc + (size_t)u * s.Fs, lane, pu);
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -505,7 +502,7 @@ void reset_counters(tsvd_model* m) {
 // Rebuild from the FP32 masters (explicit calls, Hogwild epochs).
 void rebuild_ycache(tsvd_model* m) {
     ProfScope ps(m, "rebuild_ycache");
-    const int vpl = (int)(m->d.Fs / 32);
+    const int vpl = (int)std::min<uint32_t>(m->d.Fs / 32, 8);
     TSVD_DISPATCH(vpl, launch_rebuild<V>(m, nullptr, nullptr));
     m->ycache_valid = true;
 }
@@ -516,7 +513,7 @@ void launch_rebuild_ycache(tsvd_model* m, float* pyc) {
     ProfScope ps(m, "rebuild_ycache");
     const __nv_bfloat16* ybf =
         m->opts.precision >= TSVD_PREC_BF16_READ ? m->m_bf_yfeat.as<__nv_bfloat16>() : nullptr;
-    const int vpl = (int)(m->d.Fs / 32);
+    const int vpl = (int)std::min<uint32_t>(m->d.Fs / 32, 8);
     TSVD_DISPATCH(vpl, launch_rebuild<V>(m, ybf, pyc));
     m->ycache_valid = true;
 }
@@ -530,7 +527,13 @@ void run_epoch(tsvd_model* m, uint64_t epoch) {
         TSVD_CUDA(cudaMemsetAsync(m->d.ufeat2, 0, m->m_ufeat2.bytes, m->stream));
     }
     reset_counters(m);
-    if (m->opts.schedule == TSVD_SCHED_HOGWILD || m->opts.schedule == TSVD_SCHED_SEQUENTIAL) {
+    // Tsvdx4pModel::fit_epoch runs TxModel::fit_epoch on its seq_epochs
+    // (src/tsvdx4p.rs:815-822)
+    bool seq_now = m->opts.schedule == TSVD_SCHED_SEQUENTIAL;
+    if (m->opts.schedule == TSVD_SCHED_STRATIFIED)
+        for (int k = 0; k < 5; ++k)
+            if (m->opts.seq_epochs[k] > 0 && (uint64_t)m->opts.seq_epochs[k] == epoch) seq_now = true;
+    if (m->opts.schedule == TSVD_SCHED_HOGWILD || seq_now) {
         // per-epoch user order: injected, or get_users (src/lib.rs:486-494)
         std::vector<uint32_t> order;
         auto it = m->injected_order.find(epoch);
@@ -538,8 +541,8 @@ void run_epoch(tsvd_model* m, uint64_t epoch) {
         else order = user_order(m->d.n_users, c.shuffle_users != 0, c.seed, epoch);
         TSVD_CUDA(cudaMemcpyAsync(m->m_perm.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, m->stream));
         TSVD_CUDA(cudaStreamSynchronize(m->stream));  // `order` leaves scope
-        if (m->opts.schedule == TSVD_SCHED_SEQUENTIAL || !c.low_memory) {
-            day_epoch_pass(m, m->m_perm.as<uint32_t>(), m->opts.schedule == TSVD_SCHED_SEQUENTIAL);
+        if (seq_now || !c.low_memory) {
+            day_epoch_pass(m, m->m_perm.as<uint32_t>(), seq_now);
         } else {
             ProfScope ps(m, "user_pass_hogwild");
             TSVD_DISPATCH(vpl, launch_hog_pass<V>(m, p, m->m_perm.as<uint32_t>()));

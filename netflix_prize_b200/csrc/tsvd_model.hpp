@@ -80,6 +80,9 @@ struct __align__(16) Rec {
 constexpr uint32_t kIdBits = 20, kIdMask = (1u << kIdBits) - 1u;
 constexpr uint32_t kChunkUsers = 512;  // ratings per chunk of the by-item split sums
 constexpr uint32_t kMaxBins = 64;
+// Fixed-point scale of the per-day NSVD1 delta sums: integer adds commute, so
+// the sums do not depend on the order the users' day runs finish in.
+constexpr double kDydScale = 4294967296.0;  // 2^32
 
 // Kernel arguments for one model (everything a kernel may touch).
 struct DeviceState {
@@ -118,6 +121,8 @@ struct DeviceState {
     float* e_user;   // [U]     per-user error sum / norm
     float* pyc;      // [U, Fs] p_u + ycache_u for the item stratum; shares g_user's memory,
                      //         which the delta sums have consumed by then
+    unsigned long long* dyd_fix;  // [I, Fs] low_memory = false: the epoch's yfeat_day deltas,
+                                  //         fixed point (kDydScale), added in any order
     // work lists
     const uint32_t* user_work;  // users in processing order
     const uint32_t* item_work;  // items in processing order
@@ -160,6 +165,7 @@ struct tsvd_model {
     tsvd::DevMem m_ubias, m_ibias, m_ufeat, m_ufeat2, m_ifeat, m_yfeat, m_ycache, m_yfeat_day;
     tsvd::DevMem m_alpha_u, m_but_bin, m_bit_bin, m_ybias, m_ycache_bias;
     tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
+    tsvd::DevMem m_dyd_fix;
     tsvd::DevMem m_g_user, m_e_user, m_user_work, m_item_work, m_counters;
     // BF16 read copies (precision form)
     tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_pyc, m_bf_ufeat2;
@@ -216,5 +222,29 @@ struct ProfScope {
 };
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// The calling thread's last error message, shared by every entry point
+// (tsvd_last_global_error); defined in tsvd_abi.cu.
+std::string& global_err();
+
+// Runs `f` for an extern "C" entry point: every exception becomes a status and
+// a message (on the model and the thread), none escapes the C ABI.
+template <class F>
+int guarded(const tsvd_model* m, F&& f) {
+    try {
+        f();
+        return TSVD_OK;
+    } catch (const Error& e) {
+        if (m) m->err = e.what();
+        global_err() = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        if (m) m->err = e.what();
+        global_err() = e.what();
+        return TSVD_ERR_INVALID;
+    }
+}
+
+inline void use_device(const tsvd_model* m) { TSVD_CUDA(cudaSetDevice(m->device)); }
 
 }  // namespace tsvd

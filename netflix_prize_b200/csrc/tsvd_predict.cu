@@ -3,6 +3,7 @@
 // behind calc_rmse (src/lib.rs:659-672). One warp per row; the SSE is reduced
 // in a fixed order (per-warp sums, per-block tree, then one block over the
 // block partials), so repeated calls are bitwise identical.
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -41,51 +42,63 @@ __device__ __forceinline__ void predict_row(const DeviceState& s, const PredPara
     const float bu_t = ubu + but + al * dv + bu_day + ycb;
     const float bi_t = ibi + bit + ibf;
     const float cu_t = s.cu[u] + (has ? s.cut[idx] : 0.0f);
-    float pu[VPL], p2[VPL], su[VPL], q[VPL], qf[VPL];
-    Row<VPL>::load_nc(s.ufeat + (size_t)u * Fs, lane, pu);
-    Row<VPL>::load_nc(s.ufeat2 + (size_t)u * Fs, lane, p2);
-    Row<VPL>::load_nc(s.ycache + (size_t)u * Fs, lane, su);
-    Row<VPL>::load_nc(s.ifeat + (size_t)i * Fs, lane, q);
-    Row<VPL>::load_nc(s.ifeat_freq + ((size_t)i * NF + f) * Fs, lane, qf);
     // per-day terms, low_memory = false (src/tx.rs:329-334, :692-699)
     const bool per_day = !pp.low_memory && has;
-    float pd[VPL], sd[VPL];
-    if (per_day) {
-        Row<VPL>::load_nc(s.ufeat_day + (size_t)idx * Fs, lane, pd);
-        Row<VPL>::load_nc(s.ycache_day + (size_t)idx * Fs, lane, sd);
+    // rows wider than 32 * VPL columns (n_feat > 256) are taken in slices of
+    // 32 * VPL columns; each element's arithmetic is the same
+    float part = 0.0f, mf = 0.0f, ns = 0.0f;
+    for (uint32_t c0 = 0; c0 < Fs; c0 += 32 * VPL) {
+        float pu[VPL], p2[VPL], su[VPL], q[VPL], qf[VPL];
+        Row<VPL>::load_nc(s.ufeat + (size_t)u * Fs + c0, lane, pu);
+        Row<VPL>::load_nc(s.ufeat2 + (size_t)u * Fs + c0, lane, p2);
+        Row<VPL>::load_nc(s.ycache + (size_t)u * Fs + c0, lane, su);
+        Row<VPL>::load_nc(s.ifeat + (size_t)i * Fs + c0, lane, q);
+        Row<VPL>::load_nc(s.ifeat_freq + ((size_t)i * NF + f) * Fs + c0, lane, qf);
+        float pd[VPL], sd[VPL];
+        if (per_day) {
+            Row<VPL>::load_nc(s.ufeat_day + (size_t)idx * Fs + c0, lane, pd);
+            Row<VPL>::load_nc(s.ycache_day + (size_t)idx * Fs + c0, lane, sd);
+        }
+        if (subs) {
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) {
+                const float qe = q[v] + qf[v];
+                float pe = pu[v] + dv * p2[v], se = su[v];
+                if (per_day) {
+                    pe += pd[v];
+                    se += sd[v];
+                }
+                mf += pe * qe;
+                ns += se * qe;
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) {
+                float pe = (pu[v] + su[v]) + dv * p2[v];
+                if (per_day) {
+                    pe += pd[v];
+                    pe += sd[v];
+                }
+                part += pe * (q[v] + qf[v]);
+            }
+        }
     }
     if (subs) {
-        float mf = 0.0f, ns = 0.0f;
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-            const float qe = q[v] + qf[v];
-            float pe = pu[v] + dv * p2[v], se = su[v];
-            if (per_day) {
-                pe += pd[v];
-                se += sd[v];
-            }
-            mf += pe * qe;
-            ns += se * qe;
-        }
         mf = warp_sum(mf);
         ns = warp_sum(ns);
         subs[0] = s.gbias + ubu + ibi + ibf + but + al * dv + bu_day + bit + bi_t * (cu_t - 1.0f) + ycb;
         subs[1] = mf;
         subs[2] = ns;
     } else {
-        float part = 0.0f;
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-            float pe = (pu[v] + su[v]) + dv * p2[v];
-            if (per_day) {
-                pe += pd[v];
-                pe += sd[v];
-            }
-            part += pe * (q[v] + qf[v]);
-        }
         dot = warp_sum(part);
         bias_part = s.gbias + bu_t + bi_t * cu_t;
     }
+}
+
+// u (and i) index the model's user (and item) tables; negative values arrive
+// here as large unsigned ones.
+__device__ __forceinline__ bool row_in_range(const DeviceState& s, uint32_t u, uint32_t i) {
+    return u < s.n_users && i < s.n_items;
 }
 
 template <int VPL>
@@ -97,7 +110,17 @@ __global__ void __launch_bounds__(kThreads) k_predict(DeviceState s, PredParams 
     const uint64_t warps = (uint64_t)gridDim.x * kWarps;
     for (uint64_t r = blockIdx.x * (uint64_t)kWarps + (threadIdx.x >> 5); r < n; r += warps) {
         float bp = 0.0f, dot = 0.0f, sub[3];
-        predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, subscores ? sub : nullptr);
+        const uint32_t ur = (uint32_t)u[r], ir = (uint32_t)it[r];
+        if (!row_in_range(s, ur, ir)) {
+            // an index outside the model's tables: no table is read, the row's
+            // outputs are NaN (device entry points cannot raise per row)
+            if (lane == 0) {
+                if (subscores) out[3 * r] = out[3 * r + 1] = out[3 * r + 2] = __int_as_float(0x7fc00000);
+                else out[r] = __int_as_float(0x7fc00000);
+            }
+            continue;
+        }
+        predict_row<VPL>(s, pp, ur, ir, d[r], lane, bp, dot, subscores ? sub : nullptr);
         if (lane == 0) {
             if (subscores) {
                 out[3 * r] = sub[0];
@@ -123,6 +146,7 @@ __global__ void __launch_bounds__(kThreads) k_sse(DeviceState s, PredParams pp, 
     double sse = 0.0, cnt = 0.0;
     for (uint64_t r = blockIdx.x * (uint64_t)kWarps + warp; r < n; r += warps) {
         if (is_test && is_test[r] != 0) continue;
+        if (!row_in_range(s, (uint32_t)u[r], (uint32_t)it[r])) continue;  // the host checked the rows
         float bp = 0.0f, dot = 0.0f;
         predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, nullptr);
         const float e = finish_score(s, pp, bp, dot) - target[r];
@@ -180,7 +204,7 @@ void predict_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, co
     if (n == 0) return;
     ProfScope ps(m, subscores ? "predict_subscores" : "predict");
     PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
-    const int vpl = (int)(m->d.Fs / 32);
+    const int vpl = (int)std::min<uint32_t>(m->d.Fs / 32, 8);
     unsigned grid = (unsigned)std::min<uint64_t>((n + kWarps - 1) / kWarps, 148ull * 16);
     TSVD_DISPATCH(vpl, (k_predict<V><<<grid, kThreads, 0, m->stream>>>(m->d, pp, u, i, day, offset, n, out, subscores)));
     TSVD_CUDA(cudaGetLastError());
@@ -192,7 +216,7 @@ void sse_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, const 
     tsvd_model* m = const_cast<tsvd_model*>(mc);
     ProfScope ps(m, "sse");
     PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
-    const int vpl = (int)(m->d.Fs / 32);
+    const int vpl = (int)std::min<uint32_t>(m->d.Fs / 32, 8);
     DevMem part;
     part.alloc((2 * kSseBlocks + 2) * sizeof(double));
     double* psse = part.as<double>();
@@ -277,9 +301,14 @@ __global__ void __launch_bounds__(kThreads) k_sse_tiles(DeviceState s, PredParam
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t lo = (uint64_t)blockIdx.x * kNoAllocTileRows;
     const uint64_t hi = lo + kNoAllocTileRows < n ? lo + kNoAllocTileRows : n;
-    double sse = 0.0, cnt = 0.0;
+    __shared__ double bsh[kWarps];
+    double sse = 0.0, cnt = 0.0, bad = 0.0;
     for (uint64_t r = lo + warp; r < hi; r += kWarps) {
         if (is_test && is_test[r] != 0) continue;
+        if (!row_in_range(s, (uint32_t)u[r], (uint32_t)it[r])) {
+            bad += 1.0;  // never read: counted and reported instead
+            continue;
+        }
         float bp = 0.0f, dot = 0.0f;
         predict_row<VPL>(s, pp, (uint32_t)u[r], (uint32_t)it[r], d[r], lane, bp, dot, nullptr);
         const double ed = (double)(finish_score(s, pp, bp, dot) - target[r]);
@@ -289,30 +318,43 @@ __global__ void __launch_bounds__(kThreads) k_sse_tiles(DeviceState s, PredParam
     if (lane == 0) {
         ssh[warp] = sse;
         csh[warp] = cnt;
+        bsh[warp] = bad;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double a = 0.0, c = 0.0;
+        double a = 0.0, c = 0.0, b = 0.0;
         for (int w = 0; w < kWarps; ++w) {
             a += ssh[w];
             c += csh[w];
+            b += bsh[w];
         }
+        // a tile with out-of-range rows stores minus their number as its count
         part[2 * blockIdx.x] = a;
-        part[2 * blockIdx.x + 1] = c;
+        part[2 * blockIdx.x + 1] = b > 0.0 ? -b : c;
     }
 }
 
-// Sums the tiles in order; out = {rmse, sse, count}.
+// Sums the tiles in order; out = {rmse, sse, count}, or {NaN, NaN, -rows out
+// of range} when any row's user or item index was out of range.
 __global__ void k_sse_tiles_final(const double* __restrict__ part, uint32_t tiles, double* __restrict__ out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double a = 0.0, c = 0.0;
+        double a = 0.0, c = 0.0, b = 0.0;
         for (uint32_t t = 0; t < tiles; ++t) {
-            a += part[2 * t];
-            c += part[2 * t + 1];
+            const double ct = part[2 * t + 1];
+            if (ct < 0.0) b -= ct;
+            else {
+                a += part[2 * t];
+                c += ct;
+            }
         }
-        out[0] = sqrt(a / c);
-        out[1] = a;
-        out[2] = c;
+        if (b > 0.0) {
+            out[0] = out[1] = __longlong_as_double(0x7ff8000000000000ll);
+            out[2] = -b;
+        } else {
+            out[0] = sqrt(a / c);
+            out[1] = a;
+            out[2] = c;
+        }
     }
 }
 
@@ -325,7 +367,7 @@ extern "C" int tsvd_calc_rmse_device_noalloc(const tsvd_model* m, const int32_t*
     using namespace tsvd;
     if (!m) return TSVD_ERR_INVALID;
     std::lock_guard<std::mutex> lk(m->mu);
-    try {
+    return guarded(m, [&] {
         if (!d_u || !d_i || !d_day || !d_target || !d_out) throw Error(TSVD_ERR_INVALID, "null device pointer");
         if (n == 0) throw Error(TSVD_ERR_INVALID, "no rows");
         if (n > kNoAllocMaxRows)
@@ -333,19 +375,15 @@ extern "C" int tsvd_calc_rmse_device_noalloc(const tsvd_model* m, const int32_t*
                                               " rows exceed the maximum of " + std::to_string(kNoAllocMaxRows) +
                                               " (its fixed scratch holds " + std::to_string(kNoAllocMaxTiles) +
                                               " tiles of " + std::to_string(kNoAllocTileRows) + " rows)");
-        TSVD_CUDA(cudaSetDevice(m->device));
+        use_device(m);
         double* part = noalloc_scratch(m->device);
         const uint32_t tiles = (uint32_t)((n + kNoAllocTileRows - 1) / kNoAllocTileRows);
         PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
-        const int vpl = (int)(m->d.Fs / 32);
+        const int vpl = (int)std::min<uint32_t>(m->d.Fs / 32, 8);
         TSVD_DISPATCH(vpl, (k_sse_tiles<V><<<tiles, kThreads, 0, m->stream>>>(m->d, pp, d_u, d_i, d_day, d_target,
                                                                               d_is_test, n, part)));
         k_sse_tiles_final<<<1, 32, 0, m->stream>>>(part, tiles, d_out);
         TSVD_CUDA(cudaGetLastError());
         const_cast<tsvd_model*>(m)->launches += 2;
-        return TSVD_OK;
-    } catch (const Error& e) {
-        m->err = e.what();
-        return e.status;
-    }
+    });
 }

@@ -166,7 +166,18 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     if (pr.n_users != tr.n_users) throw Error(TSVD_ERR_INVALID, "train and pr disagree on n_users");
     if (c.lr_w != 0 || c.lr_c != 0 || c.lr_w_day != 0 || c.lr_c_day != 0)
         throw Error(TSVD_ERR_UNSUPPORTED, "neighbourhood terms (tx5/tx6) are outside the tsvdx4 path");
-    if (c.n_feat < 1 || c.n_feat > 256) throw Error(TSVD_ERR_UNSUPPORTED, "n_feat must be in 1..256");
+    if (c.n_feat > (1u << 16)) throw Error(TSVD_ERR_UNSUPPORTED, "n_feat must be at most 65536");
+    if (c.n_feat > 256) {
+        // wide rows: the stratified and sequential schedules, low_memory, FP32
+        // (every tsvdx4 / tsvdx4p job above 256 factors, src/bin/tsvdx4-new.rs:19-22,
+        // src/bin/tsvdx4p-new.rs:14-19)
+        if (m->opts.schedule == TSVD_SCHED_HOGWILD)
+            throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256 runs with the stratified or sequential schedule");
+        if (!c.low_memory) throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256 is built for low_memory = true");
+        if (c.has_ordinal_head) throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256 is built without the ordinal head");
+        if (m->opts.precision != TSVD_PREC_FP32)
+            throw Error(TSVD_ERR_UNSUPPORTED, "n_feat above 256 is built for FP32 reads");
+    }
     if (c.n_time_bins < 1 || c.n_time_bins > kMaxBins) throw Error(TSVD_ERR_UNSUPPORTED, "n_time_bins must be in 1..64");
     if (c.n_freq_bins < 1 || c.n_freq_bins > kMaxBins) throw Error(TSVD_ERR_UNSUPPORTED, "n_freq_bins must be in 1..64");
     if (tr.n_users == 0 || tr.n_users > (1u << kIdBits) || tr.n_items == 0 || tr.n_items > (1u << kIdBits))
@@ -174,16 +185,18 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     if (tr.n_ratings == 0) throw Error(TSVD_ERR_INVALID, "empty training set");
     if (tr.n_ratings >= (1ull << 32) || pr.n_ratings >= (1ull << 32))
         throw Error(TSVD_ERR_UNSUPPORTED, "at most 2^32-1 ratings per set");
-    if (!c.low_memory && m->opts.schedule == TSVD_SCHED_STRATIFIED)
-        throw Error(TSVD_ERR_UNSUPPORTED,
-                    "low_memory = false (per-day NSVD1 terms) runs with the Hogwild or sequential schedule");
+    if (!c.low_memory && m->opts.precision != TSVD_PREC_FP32)
+        throw Error(TSVD_ERR_UNSUPPORTED, "BF16 read copies are built for low_memory = true");
+    for (int k = 0; k < 5; ++k) {
+        if (m->opts.seq_epochs[k] < 0) throw Error(TSVD_ERR_INVALID, "seq_epochs entries must be >= 0");
+        if (m->opts.seq_epochs[k] > 0 && m->opts.schedule != TSVD_SCHED_STRATIFIED)
+            throw Error(TSVD_ERR_INVALID, "seq_epochs belong to the stratified schedule");
+    }
     if (c.has_ordinal_head) {
         // The reference moves the 4 shared thresholds after every rating
         // (src/tx.rs:965-969), a serial chain over the whole epoch; every
-        // tsvdx4 job sets lr_t = 0, which is what is built.
-        if (m->opts.schedule == TSVD_SCHED_STRATIFIED)
-            throw Error(TSVD_ERR_UNSUPPORTED,
-                        "the ordinal head runs with the Hogwild or sequential schedule (tsvdx4p has none)");
+        // tsvdx4 job sets lr_t = 0, which every schedule runs (the thresholds
+        // then only shape the error and the prediction).
         if (c.ordinal_head.lr_t != 0.0f && m->opts.schedule != TSVD_SCHED_SEQUENTIAL)
             throw Error(TSVD_ERR_UNSUPPORTED,
                         "ordinal head with lr_t != 0 (thresholds trained per rating) needs the sequential schedule");
@@ -241,8 +254,11 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         if (tr.user_cnts[u] > 0) tum[u] /= (float)tr.user_cnts[u];
     if (dr <= 0) throw Error(TSVD_ERR_INVALID, "training dates must include a non-negative day");
 
+    // Rows padded with zeros (which every update keeps at zero): to a multiple
+    // of 32 floats up to 256 (a warp's row), of 256 above (slices of a warp's
+    // row); n_feat = 0 (bias-only jobs) keeps one all-zero 32-float row.
     const uint32_t F = (uint32_t)c.n_feat;
-    const uint32_t Fs = (F + 31) / 32 * 32;
+    const uint32_t Fs = F == 0 ? 32u : F <= 256 ? (F + 31) / 32 * 32 : (F + 255) / 256 * 256;
     s.n_users = U; s.n_items = I; s.F = F; s.Fs = Fs;
     s.T = (uint32_t)c.n_time_bins; s.NF = (uint32_t)c.n_freq_bins;
     // Heavy items run as rounds on a whole block; below the threshold a warp
@@ -259,7 +275,16 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     upload(d_tu, tr.user_idxs, R, st);
     upload(d_ti, tr.item_idxs, R, st);
     upload(d_td, tr.dates, R, st);
-    upload(d_tres, tr.residuals, R, st);
+    if (c.has_ordinal_head) {
+        // with the head the error comes from the raw rating, not the residual
+        // (src/tx.rs:965-969): the records carry the raw rating instead
+        std::vector<float> rawf(R);
+        for (uint64_t t = 0; t < R; ++t) rawf[t] = (float)tr.raw_ratings[t];
+        upload(d_tres, rawf.data(), R, st);
+        TSVD_CUDA(cudaStreamSynchronize(st));
+    } else {
+        upload(d_tres, tr.residuals, R, st);
+    }
     upload(d_pu, pr.user_idxs, P, st);
     upload(d_pi, pr.item_idxs, P, st);
     upload(d_pd, pr.dates, P, st);
@@ -464,9 +489,16 @@ void setup_params(tsvd_model* m) {
             drawn.push_back({m->m_yfeat_day.as<float>(), I, F, Fs, c.sigma_yd});
             zeros(m->m_ufeat_day, (size_t)s.n_ud * Fs * 4, st);
             zeros(m->m_ycache_day, (size_t)s.n_ud * Fs * 4, st);
+            zeros(m->m_dyd_fix, (size_t)I * Fs * 8, st);
         }
         drawn.push_back({m->m_ifeat_freq.as<float>(), (uint64_t)I * NF, F, Fs, c.sigma_iqf});
-        device_normal_tables(drawn.data(), (int)drawn.size(), c.seed, st);
+        if (F > 0) {
+            device_normal_tables(drawn.data(), (int)drawn.size(), c.seed, st);
+        } else {
+            // n_feat = 0 draws nothing (rand_array2 of an [n, 0] array)
+            for (const NormalTable& t : drawn)
+                TSVD_CUDA(cudaMemsetAsync(t.dst, 0, t.rows * t.stride * sizeof(float), st));
+        }
         zeros(m->m_ufeat2, (size_t)U * Fs * 4, st);
         zeros(m->m_ycache, (size_t)U * Fs * 4, st);
         zeros(m->m_alpha_u, U * 4, st);
@@ -506,6 +538,7 @@ void setup_params(tsvd_model* m) {
         s.ycache_bias = m->m_ycache_bias.as<float>(); s.ubias_day = m->m_ubias_day.as<float>();
         s.ufeat_day = c.low_memory ? nullptr : m->m_ufeat_day.as<float>();
         s.ycache_day = c.low_memory ? nullptr : m->m_ycache_day.as<float>();
+        s.dyd_fix = c.low_memory ? nullptr : m->m_dyd_fix.as<unsigned long long>();
         s.ibias_freq = m->m_ibias_freq.as<float>(); s.ifeat_freq = m->m_ifeat_freq.as<float>();
         s.cu = m->m_cu.as<float>(); s.cut = m->m_cut.as<float>();
         s.thresholds = m->m_thresholds.as<float>();

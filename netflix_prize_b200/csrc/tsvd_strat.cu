@@ -38,15 +38,16 @@ __global__ void k_to_bf16(const float* __restrict__ src, uint64_t rows, uint32_t
     }
 }
 
+// The item rows a user-stratum rating reads: q_i and q^f_i of frequency bin fb.
 template <int VPL, bool BF>
-__device__ __forceinline__ void item_rows(const DeviceState& s, const Bf16Copies& bf, uint32_t i, int lane,
+__device__ __forceinline__ void item_rows(const DeviceState& s, const Bf16Copies& bf, uint32_t i, uint32_t fb, int lane,
                                           float (&q)[VPL], float (&qf)[VPL]) {
     if constexpr (BF) {
         row_load_bf16<VPL>(bf.ifeat + (size_t)i * s.Fs, lane, q);
-        row_load_bf16<VPL>(bf.qf0 + (size_t)i * s.Fs, lane, qf);
+        row_load_bf16<VPL>(bf.qf0 + (size_t)i * s.Fs, lane, qf);  // BF16 copies: low_memory, bin 0
     } else {
         Row<VPL>::load_nc(s.ifeat + (size_t)i * s.Fs, lane, q);
-        Row<VPL>::load_nc(s.ifeat_freq + (size_t)i * s.NF * s.Fs, lane, qf);
+        Row<VPL>::load_nc(s.ifeat_freq + ((size_t)i * s.NF + fb) * s.Fs, lane, qf);
     }
 }
 
@@ -79,15 +80,46 @@ __device__ __forceinline__ void gather_y_ro(const DeviceState& s, const Bf16Copi
     }
 }
 
+// The ordinal head's thresholds (lane-uniform); lr_t = 0 in every stratified
+// epoch, so they are constant within it.
+__device__ __forceinline__ void load_thresholds(const DeviceState& s, float (&th)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) th[k] = s.raw ? __ldg(s.thresholds + k) : 0.0f;
+}
+
+// err of a rating: score - residual, or with the ordinal head the gradient of
+// -log P(y) in the score (src/tx.rs:963-972); `target` is then the raw rating.
+__device__ __forceinline__ float rating_err(const DeviceState& s, const float (&th)[4], float score, float target) {
+    return s.raw ? ordinal_grad(th, score, (int)target) : score - target;
+}
+
+// Fixed-point accumulation of a per-day NSVD1 delta row (red.global.add.u64).
+template <int VPL>
+__device__ __forceinline__ void dyd_add(unsigned long long* row, int lane, const float (&x)[VPL]) {
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+        const long long q = __double2ll_rn((double)x[v] * kDydScale);
+        atomicAdd(row + Row<VPL>::elem(lane, v), (unsigned long long)q);
+    }
+}
+
 // ---------------------------------------------------------------------------
-// User stratum. Item tables are read-only here; the item rows of rating j+1
-// are requested before rating j is used.
+// User stratum (fit_epoch_user, src/tsvdx4p.rs:390-639). Item tables are
+// read-only here; the item rows of rating j+1 are requested before rating j
+// is used. With DAY (low_memory = false) each run of equal dates gets its
+// su_day from yfeat_day (the run's training items, then the day's pr items,
+// :500-527), the ratings add ufeat_day and su_day to p_u(t), ufeat_day is
+// trained (:604-611), and at the run's end its error sum over
+// sqrt(day count) goes to every item of the run as a yfeat_day delta
+// (:614-622).
 // ---------------------------------------------------------------------------
-template <int VPL, bool BF>
+template <int VPL, bool BF, bool DAY>
 __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochParams p, Bf16Copies bf,
                                                          const uint32_t* __restrict__ order, uint32_t n_work) {
     const int lane = threadIdx.x & 31;
     const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
+    float th[4];
+    load_thresholds(s, th);
     for (;;) {
         uint32_t k = 0;
         if (lane == 0) k = atomicAdd(&s.counters[0], 1u);
@@ -134,28 +166,70 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
         float bb1 = lane + 32 < (int)T ? __ldcg(s.but_bin + (size_t)u * T + 32 + lane) : 0.0f;
         float sum_err = 0.0f;
         const float gb = s.gbias;
+        // the current run of equal dates (DAY)
+        float sud[DAY ? VPL : 1], seqd[DAY ? VPL : 1], pud[DAY ? VPL : 1];
+        float norm_day = 1.0f;
+        uint64_t run0 = 0, run1 = 0;
 
         for (uint64_t base = start; base < end; base += 32) {
             const uint32_t cnt = (uint32_t)(end - base < 32 ? end - base : 32);
             Rec mine{};
             if (lane < (int)cnt) mine = load_rec(s.rec + base + lane);
             float qn[VPL], qfn[VPL];
-            item_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, 0)), lane, qn, qfn);
+            {
+                const uint32_t k0 = __shfl_sync(kFull, mine.key, 0);
+                item_rows<VPL, BF>(s, bf, rec_id(k0), DAY ? rec_fbin(k0) : 0u, lane, qn, qfn);
+            }
             for (uint32_t j = 0; j < cnt; ++j) {
                 const Rec r = shfl_rec(mine, j);
                 const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+                // low_memory: training uses frequency bin 0 (src/tsvdx4p.rs:504-531);
+                // with the per-day terms, the run's bin
+                const uint32_t fb = DAY ? rec_fbin(r.key) : 0u;
+                const bool hud = r.ud < s.n_ud;
+                const uint64_t t = base + j;
+                if constexpr (DAY) {
+                    if (t == start || t > run1) {
+                        // a new run of equal dates (day_ranges, src/tx.rs:92-104)
+                        run0 = run1 = t;
+                        while (run1 + 1 < end && __ldg(&s.rec[run1 + 1].ud) == r.ud) ++run1;
+#pragma unroll
+                        for (int v = 0; v < VPL; ++v) sud[v] = seqd[v] = 0.0f;
+                        float dummy = 0.0f;
+                        gather_rows8<VPL>(s.yfeat_day, nullptr, Fs, run1 - run0 + 1,
+                                          [&](uint64_t q) { return rec_id(__ldg(&s.rec[run0 + q].key)); }, lane, sud,
+                                          dummy);
+                        float day_cnt = (float)(run1 - run0 + 1);
+                        if (p.full_su && hud) {
+                            const uint64_t off = s.ud_list_off[r.ud];
+                            const uint32_t pc = s.ud_pr_cnt[r.ud];
+                            gather_rows8<VPL>(s.yfeat_day, nullptr, Fs, pc,
+                                              [&](uint64_t q) { return __ldg(s.ud_list_item + off + q); }, lane, sud,
+                                              dummy);
+                            for (uint32_t c = 0; c < pc; ++c) day_cnt += 1.0f;
+                        }
+                        norm_day = sqrtf(day_cnt);
+#pragma unroll
+                        for (int v = 0; v < VPL; ++v) sud[v] = sud[v] / norm_day;
+                        if (p.has_ud && hud) Row<VPL>::load_cg(s.ufeat_day + (size_t)r.ud * Fs, lane, pud);
+                        else
+#pragma unroll
+                            for (int v = 0; v < VPL; ++v) pud[v] = 0.0f;
+                    }
+                }
                 float q[VPL], qf[VPL];
 #pragma unroll
                 for (int v = 0; v < VPL; ++v) {
                     q[v] = qn[v];
                     qf[v] = qfn[v];
                 }
-                if (j + 1 < cnt) item_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, j + 1)), lane, qn, qfn);
-                // low_memory: training uses frequency bin 0 (src/tsvdx4p.rs:504-531)
+                if (j + 1 < cnt) {
+                    const uint32_t k1 = __shfl_sync(kFull, mine.key, j + 1);
+                    item_rows<VPL, BF>(s, bf, rec_id(k1), DAY ? rec_fbin(k1) : 0u, lane, qn, qfn);
+                }
                 const float ib = __ldg(s.ibias + i);
                 const float bit = __ldg(s.bit_bin + (size_t)i * T + tb);
-                const float ibf = __ldg(s.ibias_freq + (size_t)i * NF);
-                const bool hud = r.ud < s.n_ud;
+                const float ibf = __ldg(s.ibias_freq + (size_t)i * NF + fb);
                 float bud = 0.0f;
                 if (lane == 0 && hud) bud = s.ubias_day[r.ud];
                 bud = __shfl_sync(kFull, bud, 0);
@@ -167,9 +241,16 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
                 const float cu_t = cuu + ct;
                 float part = 0.0f;
 #pragma unroll
-                for (int v = 0; v < VPL; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
+                for (int v = 0; v < VPL; ++v) {
+                    float pev = (pu[v] + su[v]) + dv * p2[v];
+                    if constexpr (DAY) {
+                        if (p.has_ud && hud) pev += pud[v];
+                        pev += sud[v];
+                    }
+                    part += (q[v] + qf[v]) * pev;
+                }
                 const float dot = warp_sum(part);
-                const float err = (gb + bu_t + bi_t * cu_t + dot) - r.res;
+                const float err = rating_err(s, th, gb + bu_t + bi_t * cu_t + dot, r.res);
                 ub -= p.lr_ub * err;
                 {
                     const float nb = but - p.lr_tu * err;
@@ -189,6 +270,22 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
                     seq[v] += err * qe;
                     pu[v] = pk - p.lr_u * (err * qe + p.reg_u * pk);
                     p2[v] = p2k - p.lr_u2 * (err * qe * dv + p.reg_u2 * p2k);
+                    if constexpr (DAY) {
+                        seqd[v] += err * qe;
+                        if (p.has_ud && hud) pud[v] = pud[v] - p.lr_ud * (err * qe + p.reg_ud * pud[v]);
+                    }
+                }
+                if constexpr (DAY) {
+                    if (t == run1) {
+                        // end of the run: ufeat_day back, and the run's yfeat_day
+                        // delta to each of its items (src/tsvdx4p.rs:614-622)
+                        if (p.has_ud && hud) Row<VPL>::store(s.ufeat_day + (size_t)r.ud * Fs, lane, pud);
+                        float gd[VPL];
+#pragma unroll
+                        for (int v = 0; v < VPL; ++v) gd[v] = seqd[v] / norm_day;
+                        for (uint64_t q2 = run0; q2 <= run1; ++q2)
+                            dyd_add<VPL>(s.dyd_fix + (size_t)rec_id(__ldg(&s.rec[q2].key)) * Fs, lane, gd);
+                    }
                 }
             }
         }
@@ -228,33 +325,36 @@ __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s) {
         const uint64_t a = s.chunk_lo[c];
         uint64_t b = s.chunk_lo[c + 1];
         if (b - a > kChunkUsers) b = a + kChunkUsers;
-        float acc[VPL];
+        // rows wider than 32 * VPL columns (n_feat > 256) in slices
+        for (uint32_t c0 = 0; c0 < Fs; c0 += 32 * VPL) {
+            float acc[VPL];
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
-        float eacc = 0.0f;
-        for (uint64_t base = a; base < b; base += 32) {
-            const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
-            const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&s.irec[base + lane].key)) : 0u;
-            for (uint32_t j = 0; j < cnt; j += B) {
-                float g[B][VPL], e[B];
+            for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
+            float eacc = 0.0f;
+            for (uint64_t base = a; base < b; base += 32) {
+                const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+                const uint32_t mine = lane < (int)cnt ? rec_id(__ldg(&s.irec[base + lane].key)) : 0u;
+                for (uint32_t j = 0; j < cnt; j += B) {
+                    float g[B][VPL], e[B];
 #pragma unroll
-                for (int q = 0; q < B; ++q) {
-                    const uint32_t u = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
-                    Row<VPL>::load_nc(s.g_user + (size_t)u * Fs, lane, g[q]);
-                    e[q] = __ldg(s.e_user + u);
-                }
+                    for (int q = 0; q < B; ++q) {
+                        const uint32_t u = __shfl_sync(kFull, mine, j + q < cnt ? j + q : cnt - 1);
+                        Row<VPL>::load_nc(s.g_user + (size_t)u * Fs + c0, lane, g[q]);
+                        e[q] = c0 == 0 ? __ldg(s.e_user + u) : 0.0f;
+                    }
 #pragma unroll
-                for (int q = 0; q < B; ++q) {
-                    if (j + q < cnt) {
+                    for (int q = 0; q < B; ++q) {
+                        if (j + q < cnt) {
 #pragma unroll
-                        for (int v = 0; v < VPL; ++v) acc[v] += g[q][v];
-                        eacc += e[q];
+                            for (int v = 0; v < VPL; ++v) acc[v] += g[q][v];
+                            eacc += e[q];
+                        }
                     }
                 }
             }
+            Row<VPL>::store(s.chunk_part + (size_t)c * Fs + c0, lane, acc);
+            if (lane == 0 && c0 == 0) s.chunk_epart[c] = eacc;
         }
-        Row<VPL>::store(s.chunk_part + (size_t)c * Fs, lane, acc);
-        if (lane == 0) s.chunk_epart[c] = eacc;
     }
 }
 
@@ -266,24 +366,38 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
     for (uint32_t i = blockIdx.x * kWarps + (threadIdx.x >> 5); i < s.n_items; i += warps) {
         const uint32_t c0 = s.item_chunk0[i], c1 = s.item_chunk0[i + 1];
         if (c0 == c1) continue;
-        float acc[VPL];
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
-        float eacc = 0.0f;
-        for (uint32_t c = c0; c < c1; ++c) {
-            float g[VPL];
-            Row<VPL>::load_cg(s.chunk_part + (size_t)c * Fs, lane, g);
-#pragma unroll
-            for (int v = 0; v < VPL; ++v) acc[v] += g[v];
-            eacc += __ldcg(s.chunk_epart + c);
-        }
         const float nc = (float)(s.item_off[i + 1] - s.item_off[i]);
         const float scale = p.nsvd_norm_exp == 0.0f ? 1.0f : powf(nc, p.nsvd_norm_exp);
-        float y[VPL];
-        Row<VPL>::load_cg(s.yfeat + (size_t)i * Fs, lane, y);
+        for (uint32_t x0 = 0; x0 < Fs; x0 += 32 * VPL) {
+            float acc[VPL];
 #pragma unroll
-        for (int v = 0; v < VPL; ++v) y[v] = y[v] - p.lr_y * (acc[v] / scale + p.reg_y * y[v]);
-        Row<VPL>::store(s.yfeat + (size_t)i * Fs, lane, y);
+            for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
+            for (uint32_t c = c0; c < c1; ++c) {
+                float g[VPL];
+                Row<VPL>::load_cg(s.chunk_part + (size_t)c * Fs + x0, lane, g);
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) acc[v] += g[v];
+            }
+            float y[VPL];
+            Row<VPL>::load_cg(s.yfeat + (size_t)i * Fs + x0, lane, y);
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) y[v] = y[v] - p.lr_y * (acc[v] / scale + p.reg_y * y[v]);
+            Row<VPL>::store(s.yfeat + (size_t)i * Fs + x0, lane, y);
+            if (s.dyd_fix) {
+                // per-day NSVD1 deltas, same divisor (src/tsvdx4p.rs:370-384)
+                float yd[VPL];
+                Row<VPL>::load_cg(s.yfeat_day + (size_t)i * Fs + x0, lane, yd);
+                const unsigned long long* drow = s.dyd_fix + (size_t)i * Fs + x0;
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) {
+                    const float d = (float)((double)(long long)__ldcg(drow + Row<VPL>::elem(lane, v)) / kDydScale);
+                    yd[v] = yd[v] - p.lr_yd * (d / scale + p.reg_yd * yd[v]);
+                }
+                Row<VPL>::store(s.yfeat_day + (size_t)i * Fs + x0, lane, yd);
+            }
+        }
+        float eacc = 0.0f;
+        for (uint32_t c = c0; c < c1; ++c) eacc += __ldcg(s.chunk_epart + c);
         if (lane == 0) s.ybias[i] = s.ybias[i] - p.lr_yb * (eacc / scale);
     }
 }
@@ -386,9 +500,9 @@ __device__ __forceinline__ void pe_rows(const DeviceState& s, const Bf16Copies& 
 
 // One SGD step of the item chain; qf_at(v) is this lane's v-th element of q^f[fb].
 template <int VPL, class QF>
-__device__ __forceinline__ void item_step(const EpochParams& p, float gb, float (&q)[VPL], QF&& qf_at,
-                                          const float (&pe)[VPL], float bu_t, float cu_t, float res, uint32_t tb,
-                                          uint32_t fb, int lane, ItemState& st) {
+__device__ __forceinline__ void item_step(const DeviceState& s, const EpochParams& p, const float (&th)[4], float gb,
+                                          float (&q)[VPL], QF&& qf_at, const float (&pe)[VPL], float bu_t,
+                                          float cu_t, float res, uint32_t tb, uint32_t fb, int lane, ItemState& st) {
     const float bit = __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31);
     const float ibf = __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
     const float bi_t = st.ib + bit + ibf;
@@ -399,7 +513,7 @@ __device__ __forceinline__ void item_step(const EpochParams& p, float gb, float 
         part += pe[v] * (q[v] + qfv[v]);
     }
     const float dot = warp_sum(part);
-    const float err = (gb + bu_t + bi_t * cu_t + dot) - res;
+    const float err = rating_err(s, th, gb + bu_t + bi_t * cu_t + dot, res);
     const float ec = err * cu_t;
     st.ib -= p.lr_ib * ec;
     const float nb = bit - p.lr_ti * ec;
@@ -422,11 +536,16 @@ __device__ __forceinline__ void item_step(const EpochParams& p, float gb, float 
     for (int v = 0; v < VPL; ++v) qf_at(v) = qfv[v];
 }
 
-template <int VPL, bool BF>
+// One item by one warp (fit_epoch_item, src/tsvdx4p.rs:644-762). With DAY the
+// ratings' p_u(t) also takes ufeat_day and ycache_day of the rating's day
+// (:712-719), loaded a step ahead with the user rows.
+template <int VPL, bool BF, bool DAY>
 __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf16Copies& bf, uint32_t i, int lane) {
     const uint32_t Fs = s.Fs, NF = s.NF;
     const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
     if (a == b) return;
+    float th[4];
+    load_thresholds(s, th);
     float q[VPL];
     Row<VPL>::load_cg(s.ifeat + (size_t)i * Fs, lane, q);
     ItemState st = load_item_state(s, i, lane);
@@ -441,8 +560,19 @@ __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf1
             mine = load_rec(s.irec + base + lane);
             user_scalars(s, mine, bu_l, cu_l);
         }
-        float pn[VPL], p2n[VPL];
-        pe_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, 0)), lane, pn, p2n);
+        float pn[VPL], p2n[VPL], dn[DAY ? VPL : 1], cn[DAY ? VPL : 1];
+        auto fetch = [&](uint32_t j) {
+            const uint32_t uj = rec_id(__shfl_sync(kFull, mine.key, j));
+            pe_rows<VPL, BF>(s, bf, uj, lane, pn, p2n);
+            if constexpr (DAY) {
+                const uint32_t udj = __shfl_sync(kFull, mine.ud, j);
+                if (udj < s.n_ud) {
+                    Row<VPL>::load_nc(s.ufeat_day + (size_t)udj * Fs, lane, dn);
+                    Row<VPL>::load_nc(s.ycache_day + (size_t)udj * Fs, lane, cn);
+                }
+            }
+        };
+        fetch(0);
         // the q^f row of the current rating's bin; the next rating's row is
         // loaded a step ahead when its bin differs (this rating leaves it alone)
         uint32_t fcur = rec_fbin(__shfl_sync(kFull, mine.key, 0));
@@ -453,14 +583,23 @@ __device__ void item_light(const DeviceState& s, const EpochParams& p, const Bf1
             float pe[VPL];
 #pragma unroll
             for (int v = 0; v < VPL; ++v) pe[v] = pn[v] + r.dev * p2n[v];
-            if (j + 1 < cnt) pe_rows<VPL, BF>(s, bf, rec_id(__shfl_sync(kFull, mine.key, j + 1)), lane, pn, p2n);
+            if constexpr (DAY) {
+                if (r.ud < s.n_ud) {
+#pragma unroll
+                    for (int v = 0; v < VPL; ++v) {
+                        pe[v] += dn[v];
+                        pe[v] += cn[v];
+                    }
+                }
+            }
+            if (j + 1 < cnt) fetch(j + 1);
             const float bu_t = __shfl_sync(kFull, bu_l, j), cu_t = __shfl_sync(kFull, cu_l, j);
             const uint32_t tb = rec_tbin(r.key), fb = fcur;
             const uint32_t fnext = j + 1 < cnt ? rec_fbin(__shfl_sync(kFull, mine.key, j + 1)) : fcur;
             float qfn[VPL];
             if (fnext != fcur) Row<VPL>::load_cg(qf_base + (size_t)fnext * Fs, lane, qfn);
-            item_step<VPL>(p, gb, q, [&](int v) -> float& { return qfv[v]; }, pe, bu_t, cu_t, r.res, tb, fb, lane,
-                           st);
+            item_step<VPL>(s, p, th, gb, q, [&](int v) -> float& { return qfv[v]; }, pe, bu_t, cu_t, r.res, tb, fb,
+                           lane, st);
             Row<VPL>::store(qf_base + (size_t)fcur * Fs, lane, qfv);
             if (fnext != fcur) {
 #pragma unroll
@@ -528,7 +667,7 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-template <int VPL, bool BF>
+template <int VPL, bool BF, bool DAY>
 __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, EpochParams p, Bf16Copies bf) {
     extern __shared__ __align__(16) float smem[];
     __shared__ uint32_t sh_k;
@@ -575,13 +714,13 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
         const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
         if (b - a < s.heavy_min) {
             // Items are ordered heaviest first: from here on every item is light.
-            if (warp == 0) item_light<VPL, BF>(s, p, bf, i, lane);
+            if (warp == 0) item_light<VPL, BF, DAY>(s, p, bf, i, lane);
             for (;;) {
                 uint32_t k2 = 0;
                 if (lane == 0) k2 = atomicAdd(&s.counters[2], 1u);
                 k2 = __shfl_sync(kFull, k2, 0);
                 if (k2 >= s.n_items) return;
-                item_light<VPL, BF>(s, p, bf, s.item_work[k2], lane);
+                item_light<VPL, BF, DAY>(s, p, bf, s.item_work[k2], lane);
             }
         }
         // ---------------- heavy item: whole CTA ----------------
@@ -971,6 +1110,268 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
     }
 }
 
+// ---------------------------------------------------------------------------
+// n_feat > 256 (the tsvdx4 400lm ... 4800lm jobs, tsvdx4p up to 16000): rows
+// of Fs = 256 k columns. A warp's unit keeps its own rows in global memory
+// (they are private to it, and each lane reads back only what it wrote) and
+// takes each rating in two passes over 256-column slices: the dot product,
+// then the updates. Per element the arithmetic is that of the narrow kernels.
+// ---------------------------------------------------------------------------
+constexpr int kWV = 8;                   // values per lane in a slice
+constexpr uint32_t kSlice = 32 * kWV;    // columns per slice
+
+__global__ void __launch_bounds__(kThreads) k_user_strat_wide(DeviceState s, EpochParams p,
+                                                              const uint32_t* __restrict__ order, uint32_t n_work) {
+    using R8 = Row<kWV>;
+    const int lane = threadIdx.x & 31;
+    const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
+    float th[4];
+    load_thresholds(s, th);
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(&s.counters[0], 1u);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= n_work) break;
+        const uint32_t u = order[k];
+        const uint64_t start = s.user_off[u], end = s.user_off[u + 1];
+        if (start == end) continue;
+        const uint64_t ps = s.pr_off[u], pe = s.pr_off[u + 1];
+        const uint64_t total = (end - start) + (p.full_su ? (pe - ps) : 0);
+        const float norm = sqrtf((float)total);
+        float* pu_row = s.ufeat + (size_t)u * Fs;
+        float* p2_row = s.ufeat2 + (size_t)u * Fs;
+        float* su_row = s.ycache + (size_t)u * Fs;
+        float* sq_row = s.g_user + (size_t)u * Fs;  // the NSVD1 error sum, then the user's gradient
+        float sub;
+        if (p.use_ycache) {
+            sub = __ldcg(s.ycache_bias + u);
+        } else {
+            sub = 0.0f;
+            for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                float su[kWV], sb = 0.0f;
+#pragma unroll
+                for (int v = 0; v < kWV; ++v) su[v] = 0.0f;
+                const Rec* rr = s.rec + start;
+                gather_rows8<kWV>(s.yfeat + c0, c0 == 0 ? s.ybias : nullptr, Fs, end - start,
+                                  [&](uint64_t q) { return rec_id(__ldg(&rr[q].key)); }, lane, su, sb);
+                if (p.full_su) {
+                    const uint32_t* pp = s.pr_item + ps;
+                    gather_rows8<kWV>(s.yfeat + c0, c0 == 0 ? s.ybias : nullptr, Fs, pe - ps,
+                                      [&](uint64_t q) { return __ldg(pp + q); }, lane, su, sb);
+                }
+#pragma unroll
+                for (int v = 0; v < kWV; ++v) su[v] = su[v] / norm;
+                R8::store(su_row + c0, lane, su);
+                if (c0 == 0) sub = sb / norm;
+            }
+            if (lane == 0) s.ycache_bias[u] = sub;
+        }
+        {
+            const float z[kWV] = {};
+            for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) R8::store(sq_row + c0, lane, z);
+        }
+        float ub = __ldcg(s.ubias + u), al = __ldcg(s.alpha_u + u), cuu = __ldcg(s.cu + u);
+        float bb0 = lane < (int)T ? __ldcg(s.but_bin + (size_t)u * T + lane) : 0.0f;
+        float bb1 = lane + 32 < (int)T ? __ldcg(s.but_bin + (size_t)u * T + 32 + lane) : 0.0f;
+        float sum_err = 0.0f;
+        const float gb = s.gbias;
+        for (uint64_t base = start; base < end; base += 32) {
+            const uint32_t cnt = (uint32_t)(end - base < 32 ? end - base : 32);
+            Rec mine{};
+            if (lane < (int)cnt) mine = load_rec(s.rec + base + lane);
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const Rec r = shfl_rec(mine, j);
+                const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
+                const bool hud = r.ud < s.n_ud;
+                const float* q_row = s.ifeat + (size_t)i * Fs;
+                const float* qf_row = s.ifeat_freq + (size_t)i * NF * Fs;  // low_memory: bin 0
+                const float ib = __ldg(s.ibias + i);
+                const float bit = __ldg(s.bit_bin + (size_t)i * T + tb);
+                const float ibf = __ldg(s.ibias_freq + (size_t)i * NF);
+                float bud = 0.0f;
+                if (lane == 0 && hud) bud = s.ubias_day[r.ud];
+                bud = __shfl_sync(kFull, bud, 0);
+                const float ct = hud ? __ldg(s.cut + r.ud) : 0.0f;
+                const float but = __shfl_sync(kFull, tb < 32 ? bb0 : bb1, tb & 31);
+                const float dv = r.dev;
+                const float bu_t = ub + but + al * dv + bud + sub;
+                const float bi_t = ib + bit + ibf;
+                const float cu_t = cuu + ct;
+                float part = 0.0f;
+                for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                    float q[kWV], qf[kWV], pu[kWV], su[kWV], p2[kWV];
+                    R8::load_nc(q_row + c0, lane, q);
+                    R8::load_nc(qf_row + c0, lane, qf);
+                    R8::load_cg(pu_row + c0, lane, pu);
+                    R8::load_cg(su_row + c0, lane, su);
+                    R8::load_cg(p2_row + c0, lane, p2);
+#pragma unroll
+                    for (int v = 0; v < kWV; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
+                }
+                const float dot = warp_sum(part);
+                const float err = rating_err(s, th, gb + bu_t + bi_t * cu_t + dot, r.res);
+                ub -= p.lr_ub * err;
+                {
+                    const float nb = but - p.lr_tu * err;
+                    if (lane == (int)(tb & 31)) {
+                        if (tb < 32) bb0 = nb;
+                        else bb1 = nb;
+                    }
+                }
+                al -= p.lr_ta * err * dv;
+                if (lane == 0 && hud) s.ubias_day[r.ud] = bud - p.lr_ubd * err;
+                cuu -= p.lr_cu * (err * bi_t + p.reg_cu * (cuu - 1.0f));
+                sum_err += err;
+                for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                    float q[kWV], qf[kWV], pu[kWV], p2[kWV], sq[kWV];
+                    R8::load_nc(q_row + c0, lane, q);
+                    R8::load_nc(qf_row + c0, lane, qf);
+                    R8::load_cg(pu_row + c0, lane, pu);
+                    R8::load_cg(p2_row + c0, lane, p2);
+                    R8::load_cg(sq_row + c0, lane, sq);
+#pragma unroll
+                    for (int v = 0; v < kWV; ++v) {
+                        const float qe = q[v] + qf[v];
+                        const float pk = pu[v], p2k = p2[v];
+                        sq[v] += err * qe;
+                        pu[v] = pk - p.lr_u * (err * qe + p.reg_u * pk);
+                        p2[v] = p2k - p.lr_u2 * (err * qe * dv + p.reg_u2 * p2k);
+                    }
+                    R8::store(pu_row + c0, lane, pu);
+                    R8::store(p2_row + c0, lane, p2);
+                    R8::store(sq_row + c0, lane, sq);
+                }
+            }
+        }
+        if (lane == 0) {
+            s.ubias[u] = ub;
+            s.alpha_u[u] = al;
+            s.cu[u] = cuu;
+        }
+        if (lane < (int)T) s.but_bin[(size_t)u * T + lane] = bb0;
+        if (lane + 32 < (int)T) s.but_bin[(size_t)u * T + 32 + lane] = bb1;
+        for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+            float g[kWV];
+            R8::load_cg(sq_row + c0, lane, g);
+#pragma unroll
+            for (int v = 0; v < kWV; ++v) g[v] = g[v] / norm;
+            R8::store(sq_row + c0, lane, g);
+        }
+        if (lane == 0) s.e_user[u] = sum_err / norm;
+    }
+}
+
+// Item stratum for wide rows: one warp per item, the item's q and q^f rows in
+// global memory, every item on the one-warp chain.
+__global__ void __launch_bounds__(kThreads) k_item_wide(DeviceState s, EpochParams p) {
+    using R8 = Row<kWV>;
+    const int lane = threadIdx.x & 31;
+    const uint32_t Fs = s.Fs, NF = s.NF;
+    float th[4];
+    load_thresholds(s, th);
+    const float gb = s.gbias;
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(&s.counters[2], 1u);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= s.n_items) break;
+        const uint32_t i = s.item_work[k];
+        const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
+        if (a == b) continue;
+        float* q_row = s.ifeat + (size_t)i * Fs;
+        float* qf_base = s.ifeat_freq + (size_t)i * NF * Fs;
+        ItemState st = load_item_state(s, i, lane);
+        for (uint64_t base = a; base < b; base += 32) {
+            const uint32_t cnt = (uint32_t)(b - base < 32 ? b - base : 32);
+            Rec mine{};
+            float bu_l = 0.0f, cu_l = 0.0f;
+            if (lane < (int)cnt) {
+                mine = load_rec(s.irec + base + lane);
+                user_scalars(s, mine, bu_l, cu_l);
+            }
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const Rec r = shfl_rec(mine, j);
+                const uint32_t u = rec_id(r.key), tb = rec_tbin(r.key), fb = rec_fbin(r.key);
+                const float bu_t = __shfl_sync(kFull, bu_l, j), cu_t = __shfl_sync(kFull, cu_l, j);
+                const float* pyc_row = s.pyc + (size_t)u * Fs;
+                const float* p2_row = s.ufeat2 + (size_t)u * Fs;
+                float* qf_row = qf_base + (size_t)fb * Fs;
+                const float bit = __shfl_sync(kFull, tb < 32 ? st.bt0 : st.bt1, tb & 31);
+                const float ibf = __shfl_sync(kFull, fb < 32 ? st.bf0 : st.bf1, fb & 31);
+                const float bi_t = st.ib + bit + ibf;
+                float part = 0.0f;
+                for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                    float x[kWV], y[kWV], q[kWV], qf[kWV];
+                    R8::load_nc(pyc_row + c0, lane, x);
+                    R8::load_nc(p2_row + c0, lane, y);
+                    R8::load_cg(q_row + c0, lane, q);
+                    R8::load_cg(qf_row + c0, lane, qf);
+#pragma unroll
+                    for (int v = 0; v < kWV; ++v) part += (x[v] + r.dev * y[v]) * (q[v] + qf[v]);
+                }
+                const float dot = warp_sum(part);
+                const float err = rating_err(s, th, gb + bu_t + bi_t * cu_t + dot, r.res);
+                const float ec = err * cu_t;
+                st.ib -= p.lr_ib * ec;
+                const float nb = bit - p.lr_ti * ec;
+                if (lane == (int)(tb & 31)) {
+                    if (tb < 32) st.bt0 = nb;
+                    else st.bt1 = nb;
+                }
+                const float nf = ibf - p.lr_ibf * ec;
+                if (lane == (int)(fb & 31)) {
+                    if (fb < 32) st.bf0 = nf;
+                    else st.bf1 = nf;
+                }
+                for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
+                    float x[kWV], y[kWV], q[kWV], qf[kWV];
+                    R8::load_nc(pyc_row + c0, lane, x);
+                    R8::load_nc(p2_row + c0, lane, y);
+                    R8::load_cg(q_row + c0, lane, q);
+                    R8::load_cg(qf_row + c0, lane, qf);
+#pragma unroll
+                    for (int v = 0; v < kWV; ++v) {
+                        const float pev = x[v] + r.dev * y[v];
+                        const float qi = q[v];
+                        q[v] = qi - p.lr_i * (err * pev + p.reg_i * qi);
+                        qf[v] = qf[v] - p.lr_iqf * (err * pev + p.reg_iqf * qf[v]);
+                    }
+                    R8::store(q_row + c0, lane, q);
+                    R8::store(qf_row + c0, lane, qf);
+                }
+            }
+        }
+        store_item_state(s, i, lane, st);
+    }
+}
+
+void strat_launch_wide(tsvd_model* m, const EpochParams& p) {
+    const DeviceState& s = m->d;
+    {
+        ProfScope ps(m, "user_pass_stratified");
+        unsigned g = persistent_grid(k_user_strat_wide, 0);
+        k_user_strat_wide<<<g, kThreads, 0, m->stream>>>(s, p, s.user_work, s.n_users);
+        TSVD_CUDA(cudaGetLastError());
+        m->launches++;
+    }
+    {
+        ProfScope ps(m, "y_apply");
+        unsigned g = persistent_grid(k_y_partial<kWV>, 0);
+        k_y_partial<kWV><<<g, kThreads, 0, m->stream>>>(s);
+        k_y_combine<kWV><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, p);
+        TSVD_CUDA(cudaGetLastError());
+        m->launches += 2;
+    }
+    launch_rebuild_ycache(m, s.pyc);
+    {
+        ProfScope ps(m, "item_pass");
+        unsigned g = persistent_grid(k_item_wide, 0);
+        k_item_wide<<<g, kThreads, 0, m->stream>>>(s, p);
+        TSVD_CUDA(cudaGetLastError());
+        m->launches++;
+    }
+}
+
 void to_bf16(tsvd_model* m, const float* src, uint64_t rows, uint64_t src_stride, void* dst) {
     const uint32_t Fs = m->d.Fs;
     const unsigned grid = (unsigned)std::min<uint64_t>((rows * Fs + 255) / 256, 148ull * 32);
@@ -979,13 +1380,21 @@ void to_bf16(tsvd_model* m, const float* src, uint64_t rows, uint64_t src_stride
     m->launches++;
 }
 
-template <int VPL, bool BF, bool BFU>
+// One stratified epoch (Tsvdx4pModel::fit_epoch, src/tsvdx4p.rs:815-822):
+// user stratum, NSVD1 delta sums and apply, ycache (and ycache_day) rebuild,
+// item stratum. The item stratum's whole-block path solves a round's errors
+// as a linear system, which holds for err = score - r only: with the ordinal
+// head, and with the per-day terms (which that path does not stage), every
+// item takes the one-warp chain.
+template <int VPL, bool BF, bool BFU, bool DAY>
 void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
-    const DeviceState& s = m->d;
+    DeviceState s = m->d;
+    if (DAY || s.raw) s.heavy_min = 0xffffffffu;
+    if (DAY) TSVD_CUDA(cudaMemsetAsync(s.dyd_fix, 0, (size_t)s.n_items * s.Fs * 8, m->stream));
     {
         ProfScope ps(m, "user_pass_stratified");
-        unsigned g = persistent_grid(k_user_strat<VPL, BF>, 0);
-        k_user_strat<VPL, BF><<<g, kThreads, 0, m->stream>>>(s, p, bf, s.user_work, s.n_users);
+        unsigned g = persistent_grid(k_user_strat<VPL, BF, DAY>, 0);
+        k_user_strat<VPL, BF, DAY><<<g, kThreads, 0, m->stream>>>(s, p, bf, s.user_work, s.n_users);
         TSVD_CUDA(cudaGetLastError());
         m->launches++;
     }
@@ -999,6 +1408,7 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     }
     if (BF) to_bf16(m, s.yfeat, s.n_items, s.Fs, m->m_bf_yfeat.p);
     launch_rebuild_ycache(m, s.pyc);
+    if (DAY) rebuild_ycache_day(m);
     if (BFU) {
         ProfScope ps(m, "bf16_copies");
         to_bf16(m, s.pyc, s.n_users, s.Fs, m->m_bf_pyc.p);
@@ -1007,13 +1417,14 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     {
         ProfScope ps(m, "item_pass");
         const size_t smem = (size_t)item_smem(s.Fs, s.NF).total * sizeof(float);
-        TSVD_CUDA(cudaFuncSetAttribute(k_item_pass<VPL, BFU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        auto kern = k_item_pass<VPL, BFU, DAY>;
+        TSVD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int dev = 0, sms = 0, per_sm = 0;
         TSVD_CUDA(cudaGetDevice(&dev));
         TSVD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        TSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_item_pass<VPL, BFU>, kItemThreads, smem));
+        TSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kItemThreads, smem));
         const unsigned g = (unsigned)(sms * std::max(per_sm, 1));
-        k_item_pass<VPL, BFU><<<g, kItemThreads, smem, m->stream>>>(s, p, bf);
+        kern<<<g, kItemThreads, smem, m->stream>>>(s, p, bf);
         TSVD_CUDA(cudaGetLastError());
         m->launches++;
     }
@@ -1039,10 +1450,17 @@ __global__ void k_reset_users(DeviceState s, const uint32_t* __restrict__ users,
     }
 }
 
+// (With the per-day terms the fold-in's yfeat_day deltas land in dyd_fix,
+// which the next stratified epoch clears before its user stratum.)
 template <int VPL>
 void foldin_launch(tsvd_model* m, const EpochParams& p, const uint32_t* d_users, uint32_t n) {
-    unsigned g = persistent_grid(k_user_strat<VPL, false>, 0);
-    k_user_strat<VPL, false><<<g, kThreads, 0, m->stream>>>(m->d, p, Bf16Copies{}, d_users, n);
+    if (m->d.dyd_fix) {
+        unsigned g = persistent_grid(k_user_strat<VPL, false, true>, 0);
+        k_user_strat<VPL, false, true><<<g, kThreads, 0, m->stream>>>(m->d, p, Bf16Copies{}, d_users, n);
+    } else {
+        unsigned g = persistent_grid(k_user_strat<VPL, false, false>, 0);
+        k_user_strat<VPL, false, false><<<g, kThreads, 0, m->stream>>>(m->d, p, Bf16Copies{}, d_users, n);
+    }
     TSVD_CUDA(cudaGetLastError());
     m->launches++;
 }
@@ -1067,12 +1485,16 @@ void stratified_epoch(tsvd_model* m, const EpochParams& p) {
         bf.ufeat2 = m->m_bf_ufeat2.as<__nv_bfloat16>();
     }
     const int vpl = (int)(s.Fs / 32);
-    if (prec == TSVD_PREC_FP32) {
-        TSVD_DISPATCH(vpl, (strat_launch<V, false, false>(m, p, bf)));
+    if (s.Fs > kSlice) {  // n_feat > 256: low_memory, FP32
+        strat_launch_wide(m, p);
+    } else if (s.dyd_fix) {  // low_memory = false (FP32 only)
+        TSVD_DISPATCH(vpl, (strat_launch<V, false, false, true>(m, p, bf)));
+    } else if (prec == TSVD_PREC_FP32) {
+        TSVD_DISPATCH(vpl, (strat_launch<V, false, false, false>(m, p, bf)));
     } else if (prec == TSVD_PREC_BF16_READ) {
-        TSVD_DISPATCH(vpl, (strat_launch<V, true, false>(m, p, bf)));
+        TSVD_DISPATCH(vpl, (strat_launch<V, true, false, false>(m, p, bf)));
     } else {
-        TSVD_DISPATCH(vpl, (strat_launch<V, true, true>(m, p, bf)));
+        TSVD_DISPATCH(vpl, (strat_launch<V, true, true, false>(m, p, bf)));
     }
 }
 
@@ -1081,33 +1503,14 @@ void stratified_epoch(tsvd_model* m, const EpochParams& p) {
 // ---------------------------------------------------------------------------
 // Fold-in and user reset entry points.
 // ---------------------------------------------------------------------------
-namespace {
-thread_local std::string g_fold_err;
-
-template <class F>
-int fguard(tsvd_model* m, F&& f) {
-    try {
-        f();
-        return TSVD_OK;
-    } catch (const tsvd::Error& e) {
-        if (m) m->err = e.what();
-        g_fold_err = e.what();
-        return e.status;
-    } catch (const std::exception& e) {
-        if (m) m->err = e.what();
-        g_fold_err = e.what();
-        return TSVD_ERR_INVALID;
-    }
-}
-}  // namespace
-
 extern "C" int tsvd_foldin(tsvd_model* m, const uint32_t* users, uint64_t n, uint32_t passes) {
     using namespace tsvd;
     if (!m || (!users && n)) return TSVD_ERR_INVALID;
     std::lock_guard<std::mutex> lk(m->mu);
-    return fguard(m, [&] {
+    return guarded(m, [&] {
         if (n == 0 || passes == 0) return;
         if (n >= (1ull << 32)) throw Error(TSVD_ERR_INVALID, "too many users");
+        if (m->d.Fs > kSlice) throw Error(TSVD_ERR_UNSUPPORTED, "fold-in is built for n_feat up to 256");
         for (uint64_t k = 0; k < n; ++k)
             if (users[k] >= m->d.n_users) throw Error(TSVD_ERR_INVALID, "user out of range");
         TSVD_CUDA(cudaSetDevice(m->device));
@@ -1132,7 +1535,7 @@ extern "C" int tsvd_reset_users(tsvd_model* m, const uint32_t* users, uint64_t n
     using namespace tsvd;
     if (!m || (!users && n)) return TSVD_ERR_INVALID;
     std::lock_guard<std::mutex> lk(m->mu);
-    return fguard(m, [&] {
+    return guarded(m, [&] {
         if (n == 0) return;
         for (uint64_t k = 0; k < n; ++k)
             if (users[k] >= m->d.n_users) throw Error(TSVD_ERR_INVALID, "user out of range");

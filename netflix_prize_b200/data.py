@@ -99,6 +99,30 @@ class Dataset:
     def contains_test_examples(self) -> bool:
         return bool((self.is_test != 0).any())
 
+    def transpose(self, reorder: bool) -> "Dataset":
+        """Dataset::transpose (src/lib.rs:295-405): users and items swap roles.
+        With `reorder` the ratings are stably sorted by (old item, date), which
+        is what the reference's two-pass 16-bit radix sort of the key
+        item * n_days + date produces; without it the order is kept."""
+        if reorder:
+            n_days = int(self.dates.max()) + 1
+            key = self.item_idxs.astype(np.uint64) * np.uint64(n_days) + self.dates.astype(np.uint64)
+            o = np.argsort(key.astype(np.uint32), kind="stable")
+        else:
+            o = np.arange(self.n_ratings)
+        return Dataset(
+            user_idxs=np.ascontiguousarray(self.item_idxs[o], np.int32),
+            user_cnts=self.item_cnts.copy(),
+            item_idxs=np.ascontiguousarray(self.user_idxs[o], np.int32),
+            item_cnts=self.user_cnts.copy(),
+            item_years=np.zeros(self.n_users, np.int32),
+            raw_ratings=np.ascontiguousarray(self.raw_ratings[o]),
+            residuals=np.ascontiguousarray(self.residuals[o]),
+            dates=np.ascontiguousarray(self.dates[o]),
+            is_test=np.ascontiguousarray(self.is_test[o]),
+            name=self.name, n_users=self.n_items, n_items=self.n_users, n_ratings=self.n_ratings,
+            transposed=not self.transposed)
+
     def view(self, masked: bool = False) -> TsvdDatasetView:
         v = TsvdDatasetView()
         v.user_idxs = ptr(self.user_idxs, C.c_int32)

@@ -33,9 +33,9 @@ def _p(a):
 class TxModel:
     """A device-resident timeSVD++ model (tsvdx4 / TxModel in tx4 mode)."""
 
-    def __init__(self, tr: Dataset, pr, cfg: TxConfig, schedule: int = SCHED_HOGWILD,
+    def __init__(self, tr: Dataset, pr, cfg: TxConfig, schedule: int = SCHED_STRATIFIED,
                  precision: int = PREC_FP32, nsvd_norm_exp: float = 1.0, device: int = 0,
-                 heavy_item_ratings: int = 0):
+                 heavy_item_ratings: int = 0, seq_epochs=()):
         L = load()
         self._L = L
         self.cfg = cfg
@@ -46,6 +46,10 @@ class TxModel:
         opts.nsvd_norm_exp = nsvd_norm_exp
         opts.device = device
         opts.heavy_item_ratings = heavy_item_ratings
+        if len(seq_epochs) > 5:
+            raise ValueError("at most 5 seq_epochs (Tsvdx4pConfig::seq_epochs is [usize; 5])")
+        for k, e in enumerate(seq_epochs):
+            opts.seq_epochs[k] = int(e)
         c = cfg.to_c()
         tv = tr.view()
         pv = pr.view() if isinstance(pr, MaskedDataset) else pr.view(masked=True)
@@ -127,10 +131,13 @@ class TxModel:
         return out
 
     def save_artifacts(self, model_name: str, tr_set: str, preds_dir: str):
-        """`{preds_dir}/{name}.ifeat.{tr_set}.npy` when save_ifeat (src/tx.rs:726-732)."""
+        """`{preds_dir}/{name}.ifeat.{tr_set}.npy` when save_ifeat (src/tx.rs:726-732);
+        returns the path written (the driver logs it, as the reference's teeln! does), or None."""
         if self.cfg.save_ifeat:
             path = os.path.join(preds_dir, f"{model_name}.ifeat.{tr_set}.npy")
             np.save(path, self.get_param("ifeat"))
+            return path
+        return None
 
     # -- driver-level batched helpers -----------------------------------------
     def gen_preds(self, ds: Dataset) -> np.ndarray:
@@ -159,6 +166,10 @@ class TxModel:
         self._check(self._L.tsvd_get_param(self.h, name.encode(), _p(out), n * 4))
         F = self.cfg.n_feat
         if name in ("ufeat", "ufeat2", "ifeat", "yfeat", "ycache", "ifeat_freq"):
+            if F == 0:  # bias-only models: rows without columns
+                rows = {"ifeat": self.n_items, "yfeat": self.n_items,
+                        "ifeat_freq": self.n_items * self.cfg.n_freq_bins}.get(name, self.n_users)
+                return out.reshape(rows, 0)
             return out.reshape(-1, F)
         if name == "but_bin" or name == "bit_bin":
             return out.reshape(-1, self.cfg.n_time_bins)

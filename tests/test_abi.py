@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert native.load().tsvd_abi_version() == 1
+    assert native.load().tsvd_abi_version() == 2
 
 
 def test_struct_sizes_match_c_layout():

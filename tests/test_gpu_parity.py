@@ -306,3 +306,31 @@ def test_errors_surface_as_exceptions(tiny):
         g.predict_batch(np.array([99]), np.array([0]), np.array([1]))
     with pytest.raises(TsvdError, match="1-based"):
         g.fit_epoch(tr, pr, 0)
+
+
+def test_predict_batch_device_matches_host_and_flags_out_of_range_rows(small):
+    """tsvd_predict_batch_device (device pointers, no host row checks) equals
+    the host entry point on valid rows; a row whose user or item index is out
+    of range reads no table and gets NaN."""
+    import ctypes as C
+    import torch
+    from netflix_prize_b200 import native
+    tr, pr = small
+    g = TxModel(tr, MaskedDataset(pr), lm_cfg(f=40))
+    g.fit_epoch(tr, pr, 1)
+    want = g.predict_batch(pr.user_idxs, pr.item_idxs, pr.dates)
+    u, i = pr.user_idxs.copy(), pr.item_idxs.copy()
+    u[3], i[5], u[7] = pr.n_users + 10, pr.n_items, -4
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    du, di, dd = dev(u), dev(i), dev(pr.dates)
+    out = torch.empty(pr.n_ratings, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    rc = native.load().tsvd_predict_batch_device(g.h, C.c_void_p(du.data_ptr()), C.c_void_p(di.data_ptr()),
+                                                 C.c_void_p(dd.data_ptr()), pr.n_ratings, C.c_void_p(out.data_ptr()))
+    assert rc == 0
+    g.synchronize()
+    got = out.cpu().numpy()
+    bad = np.zeros(pr.n_ratings, bool)
+    bad[[3, 5, 7]] = True
+    assert np.isnan(got[bad]).all()
+    assert np.array_equal(got[~bad], want[~bad])

@@ -58,3 +58,25 @@ def test_noalloc_rejects_rows_beyond_its_scratch():
     rc = L.tsvd_calc_rmse_device_noalloc(model.h, fake, fake, fake, fake, None, 134217729, fake)
     assert rc == 1
     assert "exceed the maximum of 134217728" in L.tsvd_last_error(model.h).decode()
+
+
+def test_noalloc_reports_out_of_range_rows_instead_of_reading_them():
+    """Device rows are not checked on the host: a user or item index outside
+    the model's tables is skipped on the device and reported as
+    {NaN, NaN, -(rows out of range)}."""
+    import torch
+    from tests.conftest import small_sets
+    tr, pr = small_sets(n_users=2000, n_items=500, n_train=120000, seed=11)
+    model = TxModel(tr, MaskedDataset(pr), run_lm(48, 1, n_time_bins=30))
+    u = pr.user_idxs.copy()
+    i = pr.item_idxs.copy()
+    held = np.nonzero(pr.is_test == 0)[0]
+    u[held[0]] = pr.n_users          # one past the last user
+    i[held[1]] = -1                  # negative item
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    tensors = (dev(u), dev(i), dev(pr.dates), dev(pr.residuals), dev(pr.is_test))
+    out = _rmse_noalloc(model, tensors, pr.n_ratings)
+    assert np.isnan(out[0]) and np.isnan(out[1]) and out[2] == -2.0
+    # the scratch keeps no trace of it: the next call on valid rows is exact
+    ok = (dev(pr.user_idxs), dev(pr.item_idxs), dev(pr.dates), dev(pr.residuals), dev(pr.is_test))
+    assert _rmse_noalloc(model, ok, pr.n_ratings)[0] == pytest.approx(model.calc_rmse(pr), rel=1e-12, abs=0.0)

@@ -264,6 +264,51 @@ int tsvd_get_user_order(const tsvd_model* m, uint64_t epoch, uint32_t* perm, uin
 int tsvd_user_order_for_seed(uint64_t n, int32_t shuffle, uint64_t seed, uint64_t epoch, uint32_t* perm);
 int tsvd_normal_stream(uint64_t seed, float sigma, uint64_t n, float* out);
 
+/* ---- sharded runs: one process per GPU --------------------------------- */
+
+/* One stratified epoch split over P processes (one per GPU), users and items
+ * in contiguous blocks, each process holding a full model (item tables and
+ * NSVD1 tables replicated, every process creating it from the same data and
+ * config). The steps of Tsvdx4pModel::fit_epoch (src/tsvdx4p.rs:815-822) with
+ * the caller's collectives between them (device buffers, e.g. NCCL):
+ *   1. tsvd_shard_user_block(own user block): the user stratum of the block's
+ *      users (fit_epoch_user, :390-639) and the block's NSVD1 delta sums per
+ *      item (NsvdDelta, :63-80): d_sums [n_items, Fs] floats (Fs = the padded
+ *      row width, tsvd_row_width), d_sums_e [n_items]; with low_memory = false
+ *      also d_dyd [n_items, Fs] int64, the yfeat_day sums in fixed point;
+ *   2. all-reduce (sum) of those three buffers over the processes;
+ *   3. all-gather of the user blocks' rows: ufeat, ufeat2, ubias, alpha_u, cu,
+ *      but_bin, and over each block's (user, day) range (tsvd_user_day_range)
+ *      ubias_day and, with low_memory = false, ufeat_day (tsvd_copy_rows);
+ *   4. tsvd_shard_apply(the summed buffers): apply_nsvd_deltas (:341-385) and
+ *      the ycache (and ycache_day) rebuild;
+ *   5. tsvd_shard_item_block(own item block): fit_epoch_item (:644-762) for
+ *      the block's items, then the end-of-epoch steps;
+ *   6. all-gather of the item blocks' rows: ifeat, ifeat_freq (rows
+ *      i * n_freq_bins ..), ibias, bit_bin, ibias_freq.
+ * Every process then holds the same model. Results equal the one-process
+ * stratified epoch up to the order of the delta additions. Stratified
+ * schedule, FP32 only. No counterpart in the reference beyond the steps
+ * cited (its parallel schedule runs on the threads of one host). */
+int tsvd_shard_user_block(tsvd_model* m, uint64_t epoch, uint32_t u_lo, uint32_t u_hi,
+                          float* d_sums, float* d_sums_e, int64_t* d_dyd);
+int tsvd_shard_apply(tsvd_model* m, const float* d_sums, const float* d_sums_e,
+                     const int64_t* d_dyd);
+int tsvd_shard_item_block(tsvd_model* m, uint32_t i_lo, uint32_t i_hi);
+/* Rows row_lo..row_hi-1 of a parameter table (names as for tsvd_get_param;
+ * an [n] vector's rows are its elements) to (to_model = 0) or from
+ * (to_model = 1) a packed device buffer of (row_hi - row_lo) x columns floats,
+ * on the model's stream, waited for. */
+int tsvd_copy_rows(tsvd_model* m, const char* name, uint64_t row_lo, uint64_t row_hi,
+                   void* d_buf, int32_t to_model);
+/* The (user, day) rows [ud_lo, ud_hi) of users u_lo..u_hi-1 (SparseUD,
+ * src/tx.rs:21-84: a user's days are contiguous). */
+int tsvd_user_day_range(const tsvd_model* m, uint32_t u_lo, uint32_t u_hi,
+                        uint64_t* ud_lo, uint64_t* ud_hi);
+/* Fs: the padded row width of the feature tables (n_feat rounded up to 32,
+ * or to 256 above 256; 32 for n_feat = 0). */
+int tsvd_row_width(const tsvd_model* m, uint32_t* out);
+
 /* ---- batched form: several variants in one persistent launch ---------- */
 
 /* A group of variants over one dataset, e.g. the lr/reg/n_feat grid of a

@@ -340,6 +340,60 @@ int tsvd_set_param(tsvd_model* m, const char* name, const void* src, uint64_t nb
     });
 }
 
+int tsvd_copy_rows(tsvd_model* m, const char* name, uint64_t row_lo, uint64_t row_hi, void* d_buf,
+                   int32_t to_model) {
+    if (!m || !name) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(m->mu);
+    return guarded(m, [&] {
+        std::string n(name);
+        ParamRef r;
+        if (!find_param(m, n, r)) throw Error(TSVD_ERR_INVALID, "unknown parameter " + n);
+        // vectors ([n] tables) are one row of n columns: index them by element
+        if (r.rows == 1) {
+            r.rows = r.cols;
+            r.cols = 1;
+            r.stride = 1;
+        }
+        if (row_lo > row_hi || row_hi > r.rows) throw Error(TSVD_ERR_INVALID, "row range out of bounds for " + n);
+        const uint64_t rows = row_hi - row_lo;
+        if (rows == 0 || r.cols == 0) return;
+        if (!d_buf) throw Error(TSVD_ERR_INVALID, "null device buffer");
+        use_device(m);
+        float* tab = r.dev + row_lo * r.stride;
+        if (to_model)
+            TSVD_CUDA(cudaMemcpy2DAsync(tab, r.stride * 4, d_buf, r.cols * 4, r.cols * 4, rows, cudaMemcpyDeviceToDevice,
+                                        m->stream));
+        else
+            TSVD_CUDA(cudaMemcpy2DAsync(d_buf, r.cols * 4, tab, r.stride * 4, r.cols * 4, rows, cudaMemcpyDeviceToDevice,
+                                        m->stream));
+        TSVD_CUDA(cudaStreamSynchronize(m->stream));
+        if (to_model && (n == "yfeat" || n == "ybias")) m->ycache_valid = false;
+    });
+}
+
+int tsvd_row_width(const tsvd_model* m, uint32_t* out) {
+    if (!m || !out) return TSVD_ERR_INVALID;
+    *out = m->d.Fs;
+    return TSVD_OK;
+}
+
+int tsvd_user_day_range(const tsvd_model* m, uint32_t u_lo, uint32_t u_hi, uint64_t* ud_lo, uint64_t* ud_hi) {
+    if (!m || !ud_lo || !ud_hi) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(m->mu);
+    return guarded(m, [&] {
+        if (u_lo > u_hi || u_hi > m->d.n_users) throw Error(TSVD_ERR_INVALID, "user range out of bounds");
+        tsvd_model* mm = const_cast<tsvd_model*>(m);
+        if (mm->h_ud_start.empty()) {
+            use_device(m);
+            mm->h_ud_start.resize((size_t)m->d.n_users + 1);
+            TSVD_CUDA(cudaMemcpy(mm->h_ud_start.data(), m->d.ud_start, mm->h_ud_start.size() * 8,
+                                 cudaMemcpyDeviceToHost));
+        }
+        *ud_lo = mm->h_ud_start[u_lo];
+        *ud_hi = mm->h_ud_start[u_hi];
+    });
+}
+
 int tsvd_rebuild_ycache(tsvd_model* m) {
     if (!m) return TSVD_ERR_INVALID;
     std::lock_guard<std::mutex> lk(m->mu);

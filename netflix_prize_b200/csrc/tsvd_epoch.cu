@@ -558,6 +558,11 @@ void run_epoch(tsvd_model* m, uint64_t epoch) {
         p.use_ycache = (c.full_su && m->ycache_valid) ? 1 : 0;
         stratified_epoch(m, p);
     }
+    finish_epoch(m);
+}
+
+void finish_epoch(tsvd_model* m) {
+    const tsvd_config& c = m->cfg;
     if (c.has_ordinal_head) {
         // OrdinalHead::enforce_sorted_with_gap at the end of the epoch
         // (src/tx.rs:1112-1114, src/lib.rs:518-525)

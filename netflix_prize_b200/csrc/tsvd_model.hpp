@@ -126,6 +126,7 @@ struct DeviceState {
     // work lists
     const uint32_t* user_work;  // users in processing order
     const uint32_t* item_work;  // items in processing order
+    uint32_t n_item_work;       // entries of item_work the item stratum takes (n_items, or a block's)
     uint32_t* counters;         // [8] dynamic work counters
     // fixed-size chunks of the by-item index (deterministic split reductions)
     uint32_t heavy_min;  // item stratum: items with at least this many ratings take a whole block
@@ -171,10 +172,13 @@ struct tsvd_model {
     tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_pyc, m_bf_ufeat2;
     tsvd::DevMem m_chunk_lo, m_item_chunk0, m_chunk_part, m_chunk_epart;
     tsvd::DevMem m_perm;          // [U] epoch order upload buffer
+    tsvd::DevMem m_shard_work;    // a sharded run's block work list (users or items)
     tsvd::DevMem m_scratch;       // predict / rmse scratch
     size_t scratch_rows = 0;
 
     std::vector<uint32_t> h_user_cnt;  // train counts (host copy)
+    std::vector<uint64_t> h_item_off;  // by-item offsets (host copy, made on first use)
+    std::vector<uint64_t> h_ud_start;  // (user, day) offsets per user (host copy, made on first use)
     std::map<uint64_t, std::vector<uint32_t>> injected_order;
 
     // profiling
@@ -201,6 +205,7 @@ void day_epoch_pass(tsvd_model* m, const uint32_t* order, bool sequential);
 void rebuild_ycache_day(tsvd_model* m);
 // epoch drivers (tsvd_epoch.cu)
 void run_epoch(tsvd_model* m, uint64_t epoch);
+void finish_epoch(tsvd_model* m);  // end-of-epoch steps shared by every schedule
 void rebuild_ycache(tsvd_model* m);
 // predictions (tsvd_predict.cu)
 void predict_device(const tsvd_model* m, const int32_t* u, const int32_t* i, const int16_t* day,

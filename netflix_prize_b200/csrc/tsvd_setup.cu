@@ -440,6 +440,7 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
                          [&](uint32_t a, uint32_t b) { return tr.user_cnts[a] > tr.user_cnts[b]; });
         upload(m->m_user_work, uw.data(), U, st);
         s.item_work = m->m_item_work.as<uint32_t>();
+        s.n_item_work = I;
         s.user_work = m->m_user_work.as<uint32_t>();
         // fixed chunks of kChunkUsers ratings per item (deterministic split sums)
         std::vector<uint64_t> clo;

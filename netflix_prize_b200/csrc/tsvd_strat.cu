@@ -15,7 +15,9 @@
 // the user rows p_u, p2_u, ycache_u of the item stratum) and widened to FP32
 // for accumulation; masters stay FP32 and are the only tables written.
 #include <algorithm>
+#include <functional>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -312,8 +314,11 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
 // (k_y_partial), then each item adds its chunk partials in chunk order and
 // applies the update (k_y_combine).
 // ---------------------------------------------------------------------------
+// Entries whose user lies outside [u_lo, u_hi) are left out (a sharded run's
+// user block; the full range otherwise). An item's entries are sorted by user,
+// so the ones kept are contiguous and keep their order.
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s) {
+__global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t u_lo, uint32_t u_hi) {
     const int lane = threadIdx.x & 31;
     const uint32_t Fs = s.Fs;
     constexpr int B = 8;  // rows in flight per warp
@@ -322,9 +327,26 @@ __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s) {
         if (lane == 0) c = atomicAdd(&s.counters[1], 1u);
         c = __shfl_sync(kFull, c, 0);
         if (c >= s.n_chunks) break;
-        const uint64_t a = s.chunk_lo[c];
+        uint64_t a = s.chunk_lo[c];
         uint64_t b = s.chunk_lo[c + 1];
         if (b - a > kChunkUsers) b = a + kChunkUsers;
+        if (u_lo != 0 || u_hi != 0xffffffffu) {
+            // the chunk's entries of users u_lo..u_hi-1 (sorted by user)
+            uint64_t lo = a, hi = b;
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (rec_id(__ldg(&s.irec[mid].key)) < u_lo) lo = mid + 1;
+                else hi = mid;
+            }
+            uint64_t lo2 = lo, hi2 = b;
+            while (lo2 < hi2) {
+                const uint64_t mid = (lo2 + hi2) >> 1;
+                if (rec_id(__ldg(&s.irec[mid].key)) < u_hi) lo2 = mid + 1;
+                else hi2 = mid;
+            }
+            a = lo;
+            b = lo2;
+        }
         // rows wider than 32 * VPL columns (n_feat > 256) in slices
         for (uint32_t c0 = 0; c0 < Fs; c0 += 32 * VPL) {
             float acc[VPL];
@@ -399,6 +421,72 @@ __global__ void __launch_bounds__(kThreads) k_y_combine(DeviceState s, EpochPara
         float eacc = 0.0f;
         for (uint32_t c = c0; c < c1; ++c) eacc += __ldcg(s.chunk_epart + c);
         if (lane == 0) s.ybias[i] = s.ybias[i] - p.lr_yb * (eacc / scale);
+    }
+}
+
+// A user block's NSVD1 delta sums per item (chunk partials added in chunk
+// order) into sums [I, Fs] and sums_e [I], instead of applying them: the
+// ranks of a sharded run add their blocks' sums before the apply.
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_y_block_sums(DeviceState s, float* __restrict__ sums,
+                                                           float* __restrict__ sums_e) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t Fs = s.Fs;
+    const uint32_t warps = gridDim.x * kWarps;
+    for (uint32_t i = blockIdx.x * kWarps + (threadIdx.x >> 5); i < s.n_items; i += warps) {
+        const uint32_t c0 = s.item_chunk0[i], c1 = s.item_chunk0[i + 1];
+        for (uint32_t x0 = 0; x0 < Fs; x0 += 32 * VPL) {
+            float acc[VPL];
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) acc[v] = 0.0f;
+            for (uint32_t c = c0; c < c1; ++c) {
+                float g[VPL];
+                Row<VPL>::load_cg(s.chunk_part + (size_t)c * Fs + x0, lane, g);
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) acc[v] += g[v];
+            }
+            Row<VPL>::store(sums + (size_t)i * Fs + x0, lane, acc);
+        }
+        float eacc = 0.0f;
+        for (uint32_t c = c0; c < c1; ++c) eacc += __ldcg(s.chunk_epart + c);
+        if (lane == 0) sums_e[i] = eacc;
+    }
+}
+
+// apply_nsvd_deltas (src/tsvdx4p.rs:341-385) of summed deltas: sums [I, Fs],
+// sums_e [I] and, with the per-day terms, the fixed-point yfeat_day sums.
+template <int VPL>
+__global__ void __launch_bounds__(kThreads) k_y_apply_sums(DeviceState s, EpochParams p,
+                                                           const float* __restrict__ sums,
+                                                           const float* __restrict__ sums_e,
+                                                           const long long* __restrict__ dyd) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t Fs = s.Fs;
+    const uint32_t warps = gridDim.x * kWarps;
+    for (uint32_t i = blockIdx.x * kWarps + (threadIdx.x >> 5); i < s.n_items; i += warps) {
+        const uint64_t ncnt = s.item_off[i + 1] - s.item_off[i];
+        if (ncnt == 0) continue;
+        const float scale = p.nsvd_norm_exp == 0.0f ? 1.0f : powf((float)ncnt, p.nsvd_norm_exp);
+        for (uint32_t x0 = 0; x0 < Fs; x0 += 32 * VPL) {
+            float acc[VPL], y[VPL];
+            Row<VPL>::load_cg(sums + (size_t)i * Fs + x0, lane, acc);
+            Row<VPL>::load_cg(s.yfeat + (size_t)i * Fs + x0, lane, y);
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) y[v] = y[v] - p.lr_y * (acc[v] / scale + p.reg_y * y[v]);
+            Row<VPL>::store(s.yfeat + (size_t)i * Fs + x0, lane, y);
+            if (dyd) {
+                float yd[VPL];
+                Row<VPL>::load_cg(s.yfeat_day + (size_t)i * Fs + x0, lane, yd);
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) {
+                    const float d = (float)((double)__ldcg(dyd + (size_t)i * Fs + x0 + Row<VPL>::elem(lane, v)) /
+                                            kDydScale);
+                    yd[v] = yd[v] - p.lr_yd * (d / scale + p.reg_yd * yd[v]);
+                }
+                Row<VPL>::store(s.yfeat_day + (size_t)i * Fs + x0, lane, yd);
+            }
+        }
+        if (lane == 0) s.ybias[i] = s.ybias[i] - p.lr_yb * (__ldcg(sums_e + i) / scale);
     }
 }
 
@@ -709,7 +797,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
         __syncthreads();
         const uint32_t k = sh_k;
         __syncthreads();
-        if (k >= s.n_items) return;
+        if (k >= s.n_item_work) return;
         const uint32_t i = s.item_work[k];
         const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
         if (b - a < s.heavy_min) {
@@ -719,7 +807,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                 uint32_t k2 = 0;
                 if (lane == 0) k2 = atomicAdd(&s.counters[2], 1u);
                 k2 = __shfl_sync(kFull, k2, 0);
-                if (k2 >= s.n_items) return;
+                if (k2 >= s.n_item_work) return;
                 item_light<VPL, BF, DAY>(s, p, bf, s.item_work[k2], lane);
             }
         }
@@ -1274,7 +1362,7 @@ __global__ void __launch_bounds__(kThreads) k_item_wide(DeviceState s, EpochPara
         uint32_t k = 0;
         if (lane == 0) k = atomicAdd(&s.counters[2], 1u);
         k = __shfl_sync(kFull, k, 0);
-        if (k >= s.n_items) break;
+        if (k >= s.n_item_work) break;
         const uint32_t i = s.item_work[k];
         const uint64_t a = s.item_off[i], b = s.item_off[i + 1];
         if (a == b) continue;
@@ -1357,7 +1445,7 @@ void strat_launch_wide(tsvd_model* m, const EpochParams& p) {
     {
         ProfScope ps(m, "y_apply");
         unsigned g = persistent_grid(k_y_partial<kWV>, 0);
-        k_y_partial<kWV><<<g, kThreads, 0, m->stream>>>(s);
+        k_y_partial<kWV><<<g, kThreads, 0, m->stream>>>(s, 0u, 0xffffffffu);
         k_y_combine<kWV><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, p);
         TSVD_CUDA(cudaGetLastError());
         m->launches += 2;
@@ -1401,7 +1489,7 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     {
         ProfScope ps(m, "y_apply");
         unsigned g = persistent_grid(k_y_partial<VPL>, 0);
-        k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s);
+        k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, 0u, 0xffffffffu);
         k_y_combine<VPL><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, p);
         TSVD_CUDA(cudaGetLastError());
         m->launches += 2;
@@ -1463,6 +1551,80 @@ void foldin_launch(tsvd_model* m, const EpochParams& p, const uint32_t* d_users,
     }
     TSVD_CUDA(cudaGetLastError());
     m->launches++;
+}
+
+// ---------------------------------------------------------------------------
+// A sharded run's steps (one process per GPU, users and items in contiguous
+// blocks): the user stratum of a user block with the block's NSVD1 delta sums,
+// the apply of the summed deltas with the cache rebuild, and the item stratum
+// of an item block. The exchanges between them are the caller's collectives.
+// ---------------------------------------------------------------------------
+template <int VPL, bool DAY>
+void shard_user_launch(tsvd_model* m, const EpochParams& p, const uint32_t* work, uint32_t n, uint32_t u_lo,
+                       uint32_t u_hi, float* sums, float* sums_e) {
+    const DeviceState& s = m->d;
+    {
+        ProfScope ps(m, "user_pass_stratified");
+        if (s.Fs > kSlice) {
+            unsigned g = persistent_grid(k_user_strat_wide, 0);
+            k_user_strat_wide<<<g, kThreads, 0, m->stream>>>(s, p, work, n);
+        } else {
+            unsigned g = persistent_grid(k_user_strat<VPL, false, DAY>, 0);
+            k_user_strat<VPL, false, DAY><<<g, kThreads, 0, m->stream>>>(s, p, Bf16Copies{}, work, n);
+        }
+        TSVD_CUDA(cudaGetLastError());
+        m->launches++;
+    }
+    ProfScope ps(m, "y_apply");
+    unsigned g = persistent_grid(k_y_partial<VPL>, 0);
+    k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, u_lo, u_hi);
+    k_y_block_sums<VPL><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, sums, sums_e);
+    TSVD_CUDA(cudaGetLastError());
+    m->launches += 2;
+}
+
+template <int VPL, bool DAY>
+void shard_item_launch(tsvd_model* m, const EpochParams& p, const uint32_t* work, uint32_t n) {
+    DeviceState s = m->d;
+    s.item_work = work;
+    s.n_item_work = n;
+    if (DAY || s.raw) s.heavy_min = 0xffffffffu;
+    ProfScope ps(m, "item_pass");
+    if (s.Fs > kSlice) {
+        unsigned g = persistent_grid(k_item_wide, 0);
+        k_item_wide<<<g, kThreads, 0, m->stream>>>(s, p);
+    } else {
+        const size_t smem = (size_t)item_smem(s.Fs, s.NF).total * sizeof(float);
+        auto kern = k_item_pass<VPL, false, DAY>;
+        TSVD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int dev = 0, sms = 0, per_sm = 0;
+        TSVD_CUDA(cudaGetDevice(&dev));
+        TSVD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        TSVD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kItemThreads, smem));
+        kern<<<(unsigned)(sms * std::max(per_sm, 1)), kItemThreads, smem, m->stream>>>(s, p, Bf16Copies{});
+    }
+    TSVD_CUDA(cudaGetLastError());
+    m->launches++;
+}
+
+// Units lo..hi-1 of a count table, heaviest first (ties by id).
+std::vector<uint32_t> block_work(uint32_t lo, uint32_t hi, const std::function<uint64_t(uint32_t)>& count) {
+    std::vector<uint32_t> w(hi - lo);
+    std::iota(w.begin(), w.end(), lo);
+    std::stable_sort(w.begin(), w.end(), [&](uint32_t a, uint32_t b) { return count(a) > count(b); });
+    return w;
+}
+
+void upload_work(tsvd_model* m, const std::vector<uint32_t>& w) {
+    if (m->m_shard_work.bytes < std::max<size_t>(w.size(), 1) * 4) m->m_shard_work.alloc(std::max<size_t>(w.size(), 1) * 4);
+    if (!w.empty())
+        TSVD_CUDA(cudaMemcpyAsync(m->m_shard_work.p, w.data(), w.size() * 4, cudaMemcpyHostToDevice, m->stream));
+    TSVD_CUDA(cudaStreamSynchronize(m->stream));  // `w` leaves scope
+}
+
+void check_shardable(const tsvd_model* m) {
+    if (m->opts.schedule != TSVD_SCHED_STRATIFIED || m->opts.precision != TSVD_PREC_FP32)
+        throw Error(TSVD_ERR_UNSUPPORTED, "a sharded run needs the stratified schedule with FP32 reads");
 }
 
 }  // namespace
@@ -1552,5 +1714,99 @@ extern "C" int tsvd_reset_users(tsvd_model* m, const uint32_t* users, uint64_t n
         k_reset_users<<<(unsigned)n, 128, 0, m->stream>>>(m->d, du.as<uint32_t>(), (uint32_t)n, dp.as<float>());
         TSVD_CUDA(cudaGetLastError());
         TSVD_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Sharded-run entry points.
+// ---------------------------------------------------------------------------
+extern "C" int tsvd_shard_user_block(tsvd_model* m, uint64_t epoch, uint32_t u_lo, uint32_t u_hi, float* d_sums,
+                                     float* d_sums_e, int64_t* d_dyd) {
+    using namespace tsvd;
+    if (!m) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(m->mu);
+    return guarded(m, [&] {
+        check_shardable(m);
+        if (epoch == 0) throw Error(TSVD_ERR_INVALID, "epoch is 1-based");
+        if (u_lo > u_hi || u_hi > m->d.n_users) throw Error(TSVD_ERR_INVALID, "user block out of range");
+        if (!d_sums || !d_sums_e || (m->d.dyd_fix && !d_dyd))
+            throw Error(TSVD_ERR_INVALID, "null delta buffer");
+        use_device(m);
+        const DeviceState& s = m->d;
+        if (epoch == m->cfg.reset_u_epoch) {
+            TSVD_CUDA(cudaMemsetAsync(s.ufeat, 0, m->m_ufeat.bytes, m->stream));
+            TSVD_CUDA(cudaMemsetAsync(s.ufeat2, 0, m->m_ufeat2.bytes, m->stream));
+        }
+        TSVD_CUDA(cudaMemsetAsync(s.counters, 0, 64, m->stream));
+        std::vector<uint32_t> w = block_work(u_lo, u_hi, [&](uint32_t u) { return (uint64_t)m->h_user_cnt[u]; });
+        upload_work(m, w);
+        EpochParams p = make_params(m);
+        p.use_ycache = (m->cfg.full_su && m->ycache_valid) ? 1 : 0;
+        if (s.dyd_fix) TSVD_CUDA(cudaMemsetAsync(s.dyd_fix, 0, (size_t)s.n_items * s.Fs * 8, m->stream));
+        const int vpl = (int)std::min<uint32_t>(s.Fs / 32, 8);
+        if (s.dyd_fix) {
+            TSVD_DISPATCH(vpl, (shard_user_launch<V, true>(m, p, m->m_shard_work.as<uint32_t>(), (uint32_t)w.size(),
+                                                          u_lo, u_hi, d_sums, d_sums_e)));
+            TSVD_CUDA(cudaMemcpyAsync(d_dyd, s.dyd_fix, (size_t)s.n_items * s.Fs * 8, cudaMemcpyDeviceToDevice,
+                                      m->stream));
+        } else {
+            TSVD_DISPATCH(vpl, (shard_user_launch<V, false>(m, p, m->m_shard_work.as<uint32_t>(), (uint32_t)w.size(),
+                                                           u_lo, u_hi, d_sums, d_sums_e)));
+        }
+        m->ycache_valid = false;  // the ycache rows of the block's users were rewritten from the current y
+        TSVD_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+extern "C" int tsvd_shard_apply(tsvd_model* m, const float* d_sums, const float* d_sums_e, const int64_t* d_dyd) {
+    using namespace tsvd;
+    if (!m) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(m->mu);
+    return guarded(m, [&] {
+        check_shardable(m);
+        if (!d_sums || !d_sums_e || (m->d.dyd_fix && !d_dyd)) throw Error(TSVD_ERR_INVALID, "null delta buffer");
+        use_device(m);
+        const DeviceState& s = m->d;
+        const EpochParams p = make_params(m);
+        const int vpl = (int)std::min<uint32_t>(s.Fs / 32, 8);
+        {
+            ProfScope ps(m, "y_apply");
+            TSVD_DISPATCH(vpl, (k_y_apply_sums<V><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(
+                                   s, p, d_sums, d_sums_e, s.dyd_fix ? (const long long*)d_dyd : nullptr)));
+            TSVD_CUDA(cudaGetLastError());
+            m->launches++;
+        }
+        launch_rebuild_ycache(m, s.pyc);
+        rebuild_ycache_day(m);
+        TSVD_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+extern "C" int tsvd_shard_item_block(tsvd_model* m, uint32_t i_lo, uint32_t i_hi) {
+    using namespace tsvd;
+    if (!m) return TSVD_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(m->mu);
+    return guarded(m, [&] {
+        check_shardable(m);
+        if (i_lo > i_hi || i_hi > m->d.n_items) throw Error(TSVD_ERR_INVALID, "item block out of range");
+        use_device(m);
+        const DeviceState& s = m->d;
+        if (m->h_item_off.empty()) {
+            m->h_item_off.resize((size_t)s.n_items + 1);
+            TSVD_CUDA(cudaMemcpy(m->h_item_off.data(), s.item_off, m->h_item_off.size() * 8, cudaMemcpyDeviceToHost));
+        }
+        TSVD_CUDA(cudaMemsetAsync(s.counters, 0, 64, m->stream));
+        std::vector<uint32_t> w =
+            block_work(i_lo, i_hi, [&](uint32_t i) { return m->h_item_off[i + 1] - m->h_item_off[i]; });
+        upload_work(m, w);
+        const EpochParams p = make_params(m);
+        const int vpl = (int)std::min<uint32_t>(s.Fs / 32, 8);
+        if (s.dyd_fix) {
+            TSVD_DISPATCH(vpl, (shard_item_launch<V, true>(m, p, m->m_shard_work.as<uint32_t>(), (uint32_t)w.size())));
+        } else {
+            TSVD_DISPATCH(vpl, (shard_item_launch<V, false>(m, p, m->m_shard_work.as<uint32_t>(), (uint32_t)w.size())));
+        }
+        TSVD_CUDA(cudaStreamSynchronize(m->stream));
+        finish_epoch(m);
     });
 }

@@ -1,9 +1,7 @@
-"""Process-group helpers for running one replica per GPU (bench.py --gpus N).
-
-The factorizer's epoch has no exchange step in this build: each rank trains an
-independent replica, so the only collectives are the timing barrier and the
-max-over-ranks of the timed duration. `device` is "cuda" on GPUs and "cpu"
-under the gloo backend (tests)."""
+"""Process-group helpers for multi-GPU runs (bench.py --gpus N): the timing
+barrier and the max-over-ranks of a timed duration. The epoch's own
+collectives are in shard.py. `device` is "cuda" on GPUs and "cpu" under the
+gloo backend (tests)."""
 from __future__ import annotations
 
 import os

@@ -39,6 +39,7 @@ class TxModel:
         L = load()
         self._L = L
         self.cfg = cfg
+        self.device = device
         self.n_users, self.n_items = tr.n_users, tr.n_items
         opts = TsvdGpuOptions()
         opts.schedule = schedule

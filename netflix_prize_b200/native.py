@@ -27,6 +27,8 @@ EXPORTED = [
     "tsvd_encoder_create", "tsvd_encoder_destroy", "tsvd_encoder_train_epoch", "tsvd_encoder_loss_grad",
     "tsvd_encoder_forward", "tsvd_encoder_apply", "tsvd_encoder_get", "tsvd_encoder_set",
     "tsvd_encoder_target_stats", "tsvd_encoder_last_error", "tsvd_foldin", "tsvd_reset_users",
+    "tsvd_shard_user_block", "tsvd_shard_apply", "tsvd_shard_item_block", "tsvd_copy_rows", "tsvd_user_day_range",
+    "tsvd_row_width",
 ]
 
 _lib = None
@@ -92,6 +94,12 @@ def load():
     L.tsvd_group_autotune.argtypes = [P, C.c_uint32, P]
     L.tsvd_group_last_error.argtypes = [P]
     L.tsvd_group_last_error.restype = C.c_char_p
+    L.tsvd_shard_user_block.argtypes = [P, C.c_uint64, C.c_uint32, C.c_uint32, P, P, P]
+    L.tsvd_shard_apply.argtypes = [P, P, P, P]
+    L.tsvd_shard_item_block.argtypes = [P, C.c_uint32, C.c_uint32]
+    L.tsvd_copy_rows.argtypes = [P, C.c_char_p, C.c_uint64, C.c_uint64, P, C.c_int32]
+    L.tsvd_user_day_range.argtypes = [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.tsvd_row_width.argtypes = [P, C.POINTER(C.c_uint32)]
     _lib = L
     return L
 

@@ -7,6 +7,8 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <vector>
 
 #include "../include/tsvdx4_cuda.h"
 #include "tx_oracle.hpp"
@@ -168,6 +170,65 @@ int orc_fit_epoch(void* p, uint64_t epoch, int schedule, float nsvd_norm_exp, ui
             }
         };
         if (h->fp64) run(*h->m64); else run(*h->m32);
+    });
+}
+
+// The parallel schedule in the steps a sharded run takes (src/tsvdx4p.rs:
+// fit_epoch_user :390-639 restricted to the users u_lo..u_hi-1, in the epoch's
+// order; apply_nsvd_deltas :341-385 of deltas summed elsewhere; fit_epoch_item
+// :644-762 restricted to items i_lo..i_hi-1). Deltas cross the boundary as
+// FP64 arrays: dy [I*F], dyb [I], dyd [I*F] (low_memory = false, else NULL),
+// nc [I].
+int orc_user_block_p(void* p, uint64_t epoch, uint64_t u_lo, uint64_t u_hi, double* dy, double* dyb, double* dyd,
+                     double* nc) {
+    Handle* h = (Handle*)p;
+    return guard([&] {
+        auto run = [&](auto& m) {
+            using M = std::remove_reference_t<decltype(m)>;
+            m.user_phase_prologue_p(epoch);
+            std::vector<uint32_t> users;
+            for (uint32_t u : m.users_for_epoch(epoch))
+                if (u >= u_lo && u < u_hi) users.push_back(u);
+            typename M::PDeltas d(m.n_items, m.cfg.n_feat, !m.cfg.low_memory);
+            m.user_phase_p(h->tr.v, h->pr.v, users, d);
+            for (size_t k = 0; k < d.dy.v.size(); ++k) dy[k] = (double)d.dy.v[k];
+            for (size_t j = 0; j < m.n_items; ++j) {
+                dyb[j] = (double)d.dyb[j];
+                nc[j] = (double)d.nc[j];
+            }
+            if (!m.cfg.low_memory)
+                for (size_t k = 0; k < d.dyd.v.size(); ++k) dyd[k] = (double)d.dyd.v[k];
+        };
+        if (h->fp64) run(*h->m64); else run(*h->m32);
+    });
+}
+
+int orc_apply_deltas_p(void* p, const double* dy, const double* dyb, const double* dyd, const double* nc,
+                       float nsvd_norm_exp) {
+    Handle* h = (Handle*)p;
+    return guard([&] {
+        auto run = [&](auto& m) {
+            using M = std::remove_reference_t<decltype(m)>;
+            using T = std::remove_reference_t<decltype(m.ubias[0])>;
+            typename M::PDeltas d(m.n_items, m.cfg.n_feat, !m.cfg.low_memory);
+            for (size_t k = 0; k < d.dy.v.size(); ++k) d.dy.v[k] = (T)dy[k];
+            for (size_t j = 0; j < m.n_items; ++j) {
+                d.dyb[j] = (T)dyb[j];
+                d.nc[j] = (uint32_t)nc[j];
+            }
+            if (!m.cfg.low_memory)
+                for (size_t k = 0; k < d.dyd.v.size(); ++k) d.dyd.v[k] = (T)dyd[k];
+            m.apply_deltas_p(h->tr.v, h->pr.v, d, nsvd_norm_exp);
+        };
+        if (h->fp64) run(*h->m64); else run(*h->m32);
+    });
+}
+
+int orc_item_block_p(void* p, uint64_t i_lo, uint64_t i_hi) {
+    Handle* h = (Handle*)p;
+    return guard([&] {
+        if (h->fp64) h->m64->item_phase_p(h->tr.v, i_lo, i_hi);
+        else h->m32->item_phase_p(h->tr.v, i_lo, i_hi);
     });
 }
 

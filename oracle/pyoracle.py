@@ -48,6 +48,10 @@ def lib():
         L.orc_normal_stream.argtypes = [C.c_uint64, C.c_float, C.c_uint64, C.c_void_p]
         L.orc_u32_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_void_p]
         L.orc_chacha_block.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_user_block_p.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]
+        L.orc_apply_deltas_p.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float]
+        L.orc_item_block_p.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
         L.orc_last_error.restype = C.c_char_p
         L.orc_time_epochs.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
         _lib = L
@@ -127,6 +131,25 @@ class OracleModel:
     def set_user_order(self, epoch: int, perm) -> None:
         p = np.ascontiguousarray(perm, np.uint32)
         _check(lib().orc_set_user_order(self.h, epoch, _p(p), len(p)))
+
+    # -- the parallel schedule in the steps of a sharded run ----------------
+    def user_block_p(self, epoch: int, u_lo: int, u_hi: int):
+        """User phase of users u_lo..u_hi-1; returns their NSVD1 deltas
+        {dy [I, F], dyb [I], dyd [I, F] or None, nc [I]} in FP64."""
+        I, F = self._tv.n_items, self.cfg.n_feat
+        dy, dyb, nc = np.zeros((I, F)), np.zeros(I), np.zeros(I)
+        dyd = None if self.cfg.low_memory else np.zeros((I, F))
+        _check(lib().orc_user_block_p(self.h, epoch, u_lo, u_hi, _p(dy), _p(dyb),
+                                      None if dyd is None else _p(dyd), _p(nc)))
+        return {"dy": dy, "dyb": dyb, "dyd": dyd, "nc": nc}
+
+    def apply_deltas_p(self, d, nsvd_norm_exp: float = 1.0):
+        arrs = [np.ascontiguousarray(d[k], np.float64) if d[k] is not None else None
+                for k in ("dy", "dyb", "dyd", "nc")]
+        _check(lib().orc_apply_deltas_p(self.h, *[None if a is None else _p(a) for a in arrs], nsvd_norm_exp))
+
+    def item_block_p(self, i_lo: int, i_hi: int):
+        _check(lib().orc_item_block_p(self.h, i_lo, i_hi))
 
     def time_epochs(self, first_epoch: int, epochs: int, schedule: int = SCHED_SEQ) -> float:
         s = C.c_double()

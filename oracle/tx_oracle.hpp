@@ -652,29 +652,64 @@ struct TxModel {
         }
     }
 
+    // The NSVD1 deltas of a set of users (one rayon chunk's NsvdDelta,
+    // src/tsvdx4p.rs:63-80).
+    struct PDeltas {
+        Mat<T> dy, dyd;
+        std::vector<T> dyb;
+        std::vector<uint32_t> nc;
+        PDeltas(size_t I, size_t F, bool day) : dy(I, F), dyd(day ? I : 0, F), dyb(I, T(0)), nc(I, 0) {}
+    };
+
     // src/tsvdx4p.rs:390-639 followed by :341-385 and the cache rebuild.
     void fit_epoch_user_p(const DataView& tr, const DataView& pr, uint64_t epoch, float nsvd_norm_exp,
                           size_t n_threads) {
         const Config c = cfg;
-        const size_t F = c.n_feat, NF = c.n_freq_bins, NT = c.n_time_bins;
-        const bool low_mem = c.low_memory, use_probe = c.full_su;
-        if (epoch == c.reset_u_epoch) {
-            ufeat.fill(T(0));
-            ufeat2.fill(T(0));
-        }
-        std::vector<size_t> offs = calc_user_offsets(tr);
+        const size_t F = c.n_feat;
+        const bool low_mem = c.low_memory;
+        user_phase_prologue_p(epoch);
         std::vector<uint32_t> users = users_for_epoch(epoch);
         n_threads = std::max<size_t>(n_threads, 1);
         size_t chunk = std::max<size_t>((users.size() + n_threads - 1) / n_threads, 1);
-        const bool has_ud = !low_mem && c.lr_ud != 0.0f;
-        Mat<T> tot_dy(n_items, F), tot_dyd(low_mem ? 0 : n_items, F);
-        std::vector<T> tot_dyb(n_items, T(0));
-        std::vector<uint32_t> tot_nc(n_items, 0);
+        PDeltas tot(n_items, F, !low_mem);
         for (size_t c0 = 0; c0 < users.size(); c0 += chunk) {
-            Mat<T> dy(n_items, F), dyd(low_mem ? 0 : n_items, F);
-            std::vector<T> dyb(n_items, T(0));
-            std::vector<uint32_t> nc(n_items, 0);
-            for (size_t ci = c0; ci < std::min(users.size(), c0 + chunk); ++ci) {
+            PDeltas d(n_items, F, !low_mem);
+            std::vector<uint32_t> part(users.begin() + c0, users.begin() + std::min(users.size(), c0 + chunk));
+            user_phase_p(tr, pr, part, d);
+            for (size_t k = 0; k < d.dy.v.size(); ++k) tot.dy.v[k] += d.dy.v[k];
+            for (size_t j = 0; j < n_items; ++j) {
+                tot.dyb[j] += d.dyb[j];
+                tot.nc[j] += d.nc[j];
+            }
+            if (!low_mem)
+                for (size_t k = 0; k < d.dyd.v.size(); ++k) tot.dyd.v[k] += d.dyd.v[k];
+        }
+        apply_deltas_p(tr, pr, tot, nsvd_norm_exp);
+    }
+
+    // The epoch-start reset of the user factors (src/tsvdx4p.rs:401-404).
+    void user_phase_prologue_p(uint64_t epoch) {
+        if (epoch == cfg.reset_u_epoch) {
+            ufeat.fill(T(0));
+            ufeat2.fill(T(0));
+        }
+    }
+
+    // The user phase for `users` in the given order, accumulating their NSVD1
+    // deltas into d (src/tsvdx4p.rs:449-630, one chunk's loop).
+    void user_phase_p(const DataView& tr, const DataView& pr, const std::vector<uint32_t>& users, PDeltas& d) {
+        const Config c = cfg;
+        const size_t F = c.n_feat, NF = c.n_freq_bins;
+        const bool low_mem = c.low_memory, use_probe = c.full_su;
+        (void)pr;
+        std::vector<size_t> offs = calc_user_offsets(tr);
+        const bool has_ud = !low_mem && c.lr_ud != 0.0f;
+        Mat<T>& dy = d.dy;
+        Mat<T>& dyd = d.dyd;
+        std::vector<T>& dyb = d.dyb;
+        std::vector<uint32_t>& nc = d.nc;
+        {
+            for (size_t ci = 0; ci < users.size(); ++ci) {
                 const size_t u = users[ci];
                 const size_t start = offs[u], end = offs[u + 1], cnt = end - start;
                 if (cnt == 0) continue;
@@ -786,15 +821,19 @@ struct TxModel {
                     nc[j] += 1;
                 }
             }
-            for (size_t k = 0; k < dy.v.size(); ++k) tot_dy.v[k] += dy.v[k];
-            for (size_t j = 0; j < n_items; ++j) {
-                tot_dyb[j] += dyb[j];
-                tot_nc[j] += nc[j];
-            }
-            if (!low_mem)
-                for (size_t k = 0; k < dyd.v.size(); ++k) tot_dyd.v[k] += dyd.v[k];
         }
-        (void)NT;
+    }
+
+    // apply_nsvd_deltas (src/tsvdx4p.rs:341-385) of the summed deltas, then
+    // the cache rebuild (:636-638).
+    void apply_deltas_p(const DataView& tr, const DataView& pr, const PDeltas& tot, float nsvd_norm_exp) {
+        const Config c = cfg;
+        const size_t F = c.n_feat;
+        const bool low_mem = c.low_memory;
+        const Mat<T>& tot_dy = tot.dy;
+        const Mat<T>& tot_dyd = tot.dyd;
+        const std::vector<T>& tot_dyb = tot.dyb;
+        const std::vector<uint32_t>& tot_nc = tot.nc;
         const float ex = nsvd_norm_exp;
         for (size_t j = 0; j < n_items; ++j) {
             if (tot_nc[j] == 0) continue;
@@ -819,13 +858,16 @@ struct TxModel {
     }
 
     // src/tsvdx4p.rs:644-762
-    void fit_epoch_item_p(const DataView& tr) {
+    void fit_epoch_item_p(const DataView& tr) { item_phase_p(tr, 0, n_items); }
+
+    // The item phase for items i_lo..i_hi-1.
+    void item_phase_p(const DataView& tr, size_t i_lo, size_t i_hi) {
         const Config c = cfg;
         const size_t F = c.n_feat, NF = c.n_freq_bins;
         const bool low_mem = c.low_memory;
         if (by_item.starts.empty()) build_by_item(tr);
         std::vector<T> pe(F);
-        for (size_t i = 0; i < n_items; ++i) {
+        for (size_t i = i_lo; i < i_hi; ++i) {
             for (size_t e = by_item.starts[i]; e < by_item.starts[i + 1]; ++e) {
                 const size_t u = by_item.user[e], t = by_item.rating[e];
                 const T r = (T)tr.residuals[t];

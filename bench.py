@@ -58,6 +58,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttr", action="store_true", help="skip the fold-in time-to-RMSE comparison")
     ap.add_argument("--sample-users", type=int, default=20000, help="users in the CPU sample")
+    ap.add_argument("--no-train-ttr", action="store_true",
+                    help="skip the training time to the reference's held-out RMSE")
+    ap.add_argument("--batched", type=int, default=0, metavar="EPOCHS",
+                    help="also time the 16 C3 variants trained together against one after another")
     return ap.parse_args()
 
 
@@ -292,9 +296,104 @@ def time_to_rmse(model, tr, pr):
             "chosen": {"form": "encoder init + fold-in passes", "passes": w[0], "ms": w[1], "rmse": w[2]}
             if w else None,
             "chosen_over_plain_time": (w[1] / p[1]) if (p and w and p[1] > 0) else None,
+            "chosen_with_encoder_training_ms": (enc_s * 1000.0 + w[1]) if w else None,
+            "chosen_with_encoder_training_over_plain_time": ((enc_s * 1000.0 + w[1]) / p[1])
+            if (p and w and p[1] > 0) else None,
+            "fold_in_batches_for_half_the_plain_time":
+            (enc_s * 1000.0 / (0.5 * p[1] - w[1])) if (p and w and 0.5 * p[1] > w[1]) else None,
             "encoder_train_s": enc_s, "encoder_loss_first_last": [losses[0], losses[-1]],
             "plain_curve": [[k, round(ms, 3), r] for k, ms, r in plain],
             "chosen_curve": [[k, round(ms, 3), r] for k, ms, r in warm]}
+
+
+def train_to_reference_rmse(tr, pr, cfg, device: int, shape: str):
+    """Wall time of the plain GPU form to reach the reference's held-out RMSE
+    (the best epoch of the oracle's sequential TxModel curve committed under
+    tests/golden, + 0.001) from the standard init, epoch by epoch with the
+    stratified schedule. Host wall clock around the synchronous calls; the
+    per-epoch RMSE evaluations are timed apart."""
+    path = os.path.join(ROOT, "tests", "golden", f"rmse_curve_{shape}_f{cfg.n_feat}.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        ref = json.load(fh)
+    eps = ref["epochs"]
+    best = min(eps, key=lambda r: r["heldout_rmse"])
+    target = best["heldout_rmse"] + 0.001
+    from netflix_prize_b200.data import MaskedDataset
+    from netflix_prize_b200.model import TxModel
+    m = TxModel(tr, MaskedDataset(pr), cfg.replace(n_epochs=len(eps)), device=device)
+    train_ms = eval_ms = 0.0
+    curve = []
+    for e in range(1, len(eps) + 1):
+        t = time.perf_counter()
+        m.fit_epoch(tr, pr, e)
+        m.synchronize()
+        train_ms += (time.perf_counter() - t) * 1000.0
+        t = time.perf_counter()
+        r = m.calc_rmse(pr)
+        eval_ms += (time.perf_counter() - t) * 1000.0
+        curve.append([e, r, eps[e - 1]["heldout_rmse"]])
+        if r <= target:
+            break
+    m.close()
+    reached = curve[-1][1] <= target
+    return {"target_rmse": target, "target_rule": "reference best held-out RMSE + 0.001",
+            "reference": {"best_epoch": best["epoch"], "best_rmse": best["heldout_rmse"],
+                          "epochs_in_curve": len(eps), "algorithm": ref["algorithm"]},
+            "plain": {"reached": reached, "epochs": curve[-1][0], "train_ms": train_ms, "eval_ms": eval_ms},
+            "curve_gpu_vs_reference": curve}
+
+
+def c3_variants(base):
+    """The batched configuration: f in {32, 64, 128, 256} x lr in {0.003,
+    0.007} x reg in {0.005, 0.015}; lr sets lr_u and lr_i, reg sets reg_u and
+    reg_i."""
+    out = []
+    for f in (32, 64, 128, 256):
+        for lr in (0.003, 0.007):
+            for reg in (0.005, 0.015):
+                out.append(base.replace(n_feat=f, lr_u=lr, lr_i=lr, reg_u=reg, reg_i=reg))
+    return out
+
+
+def batched_leg(tr, pr, base_cfg, device: int, epochs: int):
+    """The 16 C3 variants trained together (one graph per epoch, the
+    autotuned whole-CTA thresholds) against the same variants trained one
+    after another (CUDA events around each variant's epochs)."""
+    import torch
+    from netflix_prize_b200.data import MaskedDataset
+    from netflix_prize_b200.model import TxGroup, TxModel
+    cfgs = c3_variants(base_cfg.replace(n_epochs=epochs + 1))
+    g = TxGroup(tr, MaskedDataset(pr), cfgs, device=device)
+    thr = [int(x) for x in g.autotune()]
+    g.fit_epoch(1)  # uncaptured first epoch
+    group_ms = 0.0
+    for e in range(2, epochs + 2):
+        g.fit_epoch(e)
+        group_ms += g.last_epoch_ms()
+    rmse_group = [m.calc_rmse(pr) for m in g.models]
+    g.close()
+    sep_ms = 0.0
+    for k, c in enumerate(cfgs):
+        m = TxModel(tr, MaskedDataset(pr), c, device=device, heavy_item_ratings=min(thr[k], 2**31 - 1))
+        m.fit_epoch(tr, pr, 1)
+        m.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s = torch.cuda.current_stream()
+        m.set_stream(s.cuda_stream)
+        e0.record(s)
+        for e in range(2, epochs + 2):
+            m.fit_epoch(tr, pr, e)
+        e1.record(s)
+        torch.cuda.synchronize()
+        sep_ms += e0.elapsed_time(e1)
+        m.close()
+    R = tr.n_ratings
+    return {"variants": len(cfgs), "epochs_timed": epochs, "group_ms_per_epoch": group_ms / epochs,
+            "separate_ms_per_epoch": sep_ms / epochs, "speedup": sep_ms / group_ms,
+            "group_rating_updates_per_s": R * len(cfgs) * epochs / (group_ms / 1000.0),
+            "whole_cta_thresholds": thr, "heldout_rmse_group": rmse_group}
 
 
 def main():
@@ -383,6 +482,12 @@ def main():
     if world == 1 and not args.no_ttr:
         ttr = time_to_rmse(model, tr, pr)
     del model
+    train_ttr = None
+    if world == 1 and not args.no_train_ttr:
+        train_ttr = train_to_reference_rmse(tr, pr, cfg, local, args.shape)
+    batched = None
+    if world == 1 and args.batched > 0:
+        batched = batched_leg(tr, pr, cfg, local, args.batched)
 
     # ---------------- e2e: through the C ABI from pinned host buffers ----------------
     e2e = None
@@ -437,6 +542,8 @@ def main():
         "gpu_launches": launches,
         "e2e": e2e,
         "time_to_rmse": ttr,
+        "time_to_reference_rmse": train_ttr,
+        "batched": batched,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)

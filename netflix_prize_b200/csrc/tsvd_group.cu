@@ -1,14 +1,24 @@
 // Batched form: several tsvdx4 variants (different factor sizes, learning
 // rates, regularisers) trained together over one device copy of the data.
 //
-// Every epoch is one persistent launch over (variant, user) work units plus
-// one batched ycache rebuild, captured once as a CUDA graph and replayed.
-// Each variant runs its own Hogwild epoch (its own get_users order,
-// src/lib.rs:486-494); units of the same position in the variants' orders are
-// adjacent, and users with many ratings are moved to the front so the longest
-// serial chains start first. The prefetch depth of the Hogwild ring is chosen
-// per feature width by an autotuner that times candidate depths on throwaway
-// copies of the parameters.
+// Hogwild variants: every epoch is one persistent launch over (variant, user)
+// work units plus one batched ycache rebuild, captured once as a CUDA graph
+// and replayed. Each variant runs its own Hogwild epoch (its own get_users
+// order, src/lib.rs:486-494); units of the same position in the variants'
+// orders are adjacent, and users with many ratings are moved to the front so
+// the longest serial chains start first. The prefetch depth of the Hogwild
+// ring is chosen per feature width by an autotuner that times candidate depths
+// on throwaway copies of the parameters.
+//
+// Stratified variants (the deterministic schedule, src/tsvdx4p.rs:815-822):
+// every variant's epoch runs on its own stream, forked from and joined back
+// to the group's stream, and the whole epoch of all variants is captured once
+// as one CUDA graph. A variant's item stratum is bounded by the serial chains
+// of its most-rated items, which hold a few SMs; the other variants' strata
+// fill the rest of the GPU meanwhile. The autotuner picks, per feature width,
+// which items run as whole-CTA tiles (rounds of 32 ratings solved together on
+// the tensor cores) and which run one warp each, by timing candidate
+// thresholds on throwaway copies.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -38,6 +48,8 @@ struct tsvd_group {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
+    bool stratified = false;
+    std::vector<cudaEvent_t> fork, join;  // per variant (stratified)
     uint64_t epochs_run = 0;
     uint64_t launches = 0;
     double last_epoch_ms = 0.0;
@@ -150,6 +162,103 @@ void enqueue_epoch(tsvd_group* g) {
     tsvd::launch_rebuild_batched(st, g->d_states.as<tsvd::DeviceState>(), n, U);
 }
 
+// Every variant's stratified epoch on its own stream, forked from and joined
+// to the group's stream.
+void enqueue_strat_epoch(tsvd_group* g, uint64_t epoch) {
+    for (size_t k = 0; k < g->models.size(); ++k) {
+        tsvd_model* m = g->models[k];
+        TSVD_CUDA(cudaEventRecord(g->fork[k], g->stream));
+        TSVD_CUDA(cudaStreamWaitEvent(m->stream, g->fork[k], 0));
+        tsvd::run_epoch(m, epoch);
+        TSVD_CUDA(cudaEventRecord(g->join[k], m->stream));
+        TSVD_CUDA(cudaStreamWaitEvent(g->stream, g->join[k], 0));
+    }
+}
+
+void drop_graph(tsvd_group* g) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    g->exec = nullptr;
+    g->graph = nullptr;
+}
+
+// One epoch of stratified variants. The reset epoch of any variant (which
+// zeroes that variant's user factors first), the first epoch, and runs with
+// the ordinal head (whose epoch end waits on the host) or with kernel
+// profiling are launched directly; the others replay one captured graph.
+void strat_group_epoch(tsvd_group* g, uint64_t epoch) {
+    bool direct = !g->use_graph || g->epochs_run == 0;
+    for (auto* m : g->models)
+        direct = direct || epoch == m->cfg.reset_u_epoch || m->cfg.has_ordinal_head || m->profiling;
+    if (direct) {
+        enqueue_strat_epoch(g, epoch);
+        return;
+    }
+    if (!g->exec) {
+        TSVD_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue_strat_epoch(g, epoch);
+        } catch (...) {
+            cudaGraph_t dropped = nullptr;
+            cudaStreamEndCapture(g->stream, &dropped);
+            if (dropped) cudaGraphDestroy(dropped);
+            throw;
+        }
+        TSVD_CUDA(cudaStreamEndCapture(g->stream, &g->graph));
+        TSVD_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    }
+    TSVD_CUDA(cudaGraphLaunch(g->exec, g->stream));
+}
+
+// Per feature width, the whole-CTA threshold of the item stratum that runs a
+// stratified epoch fastest (CUDA events, best of two after a warm-up), timed
+// on a throwaway variant with fresh parameters.
+void strat_autotune(tsvd_group* g, int32_t* chosen) {
+    tsvd_model* m0 = g->models[0];
+    const uint32_t cands[] = {0xffffffffu, 65536u, 32768u, 16384u, 8192u, 4096u};
+    std::vector<uint32_t> best_for(9, m0->d.heavy_min);
+    for (uint32_t vpl = 1; vpl <= 8; ++vpl) {
+        const tsvd_model* rep = nullptr;
+        for (auto* m : g->models)
+            if (m->d.Fs / 32 == vpl) {
+                rep = m;
+                break;
+            }
+        if (!rep) continue;
+        std::unique_ptr<tsvd_model, void (*)(tsvd_model*)> tmp(make_variant(m0, rep->cfg), tsvd_destroy);
+        const uint64_t ep = rep->cfg.reset_u_epoch == 1000000 ? 1000001 : 1000000;
+        double best = 1e30;
+        for (uint32_t thr : cands) {
+            tmp->d.heavy_min = thr;
+            double t_best = 1e30;
+            for (int rep_i = 0; rep_i < 3; ++rep_i) {
+                cudaEvent_t e0, e1;
+                TSVD_CUDA(cudaEventCreate(&e0));
+                TSVD_CUDA(cudaEventCreate(&e1));
+                TSVD_CUDA(cudaEventRecord(e0, tmp->stream));
+                tsvd::run_epoch(tmp.get(), ep);
+                TSVD_CUDA(cudaEventRecord(e1, tmp->stream));
+                TSVD_CUDA(cudaStreamSynchronize(tmp->stream));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (rep_i > 0) t_best = std::min<double>(t_best, ms);  // the first run warms up
+            }
+            if (t_best < best) {
+                best = t_best;
+                best_for[vpl] = thr;
+            }
+        }
+    }
+    for (size_t k = 0; k < g->models.size(); ++k) {
+        tsvd_model* m = g->models[k];
+        m->d.heavy_min = best_for[m->d.Fs / 32];
+        if (chosen) chosen[k] = (int32_t)std::min<uint32_t>(m->d.heavy_min, 0x7fffffffu);
+    }
+    drop_graph(g);  // the captured graph baked in the old thresholds
+}
+
 }  // namespace
 
 extern "C" {
@@ -164,8 +273,12 @@ int tsvd_group_create(const tsvd_config* cfgs, uint32_t n_models, const tsvd_gpu
         tsvd_gpu_options o{};
         if (opts) o = *opts;
         else o.nsvd_norm_exp = 1.0f;
-        if (o.schedule != TSVD_SCHED_HOGWILD || o.precision != TSVD_PREC_FP32)
-            throw Error(TSVD_ERR_UNSUPPORTED, "the batched form runs Hogwild epochs in FP32");
+        if ((o.schedule != TSVD_SCHED_HOGWILD && o.schedule != TSVD_SCHED_STRATIFIED) ||
+            o.precision != TSVD_PREC_FP32)
+            throw Error(TSVD_ERR_UNSUPPORTED, "the batched form runs Hogwild or stratified epochs in FP32");
+        for (int k = 0; k < 5; ++k)
+            if (o.seq_epochs[k] != 0) throw Error(TSVD_ERR_UNSUPPORTED, "the batched form has no seq_epochs");
+        g->stratified = o.schedule == TSVD_SCHED_STRATIFIED;
         for (uint32_t k = 1; k < n_models; ++k) check_compatible(cfgs[0], cfgs[k]);
         tsvd_model* m0 = nullptr;
         int r0 = tsvd_create(&cfgs[0], &o, tr, pr, &m0);
@@ -187,6 +300,14 @@ int tsvd_group_create(const tsvd_config* cfgs, uint32_t n_models, const tsvd_gpu
         const double mean = (double)m0->d.n_train / std::max<uint32_t>(1, U);
         g->heavy_min = (uint32_t)std::max(64.0, 8.0 * mean);
         g->ring_floats = ring_floats_for(g->models);
+        if (g->stratified) {
+            g->fork.resize(n_models, nullptr);
+            g->join.resize(n_models, nullptr);
+            for (uint32_t k = 0; k < n_models; ++k) {
+                TSVD_CUDA(cudaEventCreateWithFlags(&g->fork[k], cudaEventDisableTiming));
+                TSVD_CUDA(cudaEventCreateWithFlags(&g->join[k], cudaEventDisableTiming));
+            }
+        }
     });
     if (rc != TSVD_OK) {
         tsvd_group_destroy(g);
@@ -202,6 +323,10 @@ void tsvd_group_destroy(tsvd_group* g) {
     if (g->stream) cudaStreamSynchronize(g->stream);
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
+    for (cudaEvent_t e : g->fork)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : g->join)
+        if (e) cudaEventDestroy(e);
     for (size_t k = g->models.size(); k-- > 1;) tsvd_destroy(g->models[k]);  // variants borrow models[0]'s data
     if (!g->models.empty()) tsvd_destroy(g->models[0]);
     if (g->h_units) cudaFreeHost(g->h_units);
@@ -244,11 +369,30 @@ int tsvd_group_fit_epoch(tsvd_group* g, uint64_t epoch) {
                 TSVD_CUDA(cudaMemsetAsync(m->d.ufeat2, 0, m->m_ufeat2.bytes, g->stream));
             }
         }
-        build_units(g, epoch);
-        upload_tables(g);
         cudaEvent_t e0, e1;
         TSVD_CUDA(cudaEventCreate(&e0));
         TSVD_CUDA(cudaEventCreate(&e1));
+        if (g->stratified) {
+            TSVD_CUDA(cudaEventRecord(e0, g->stream));
+            try {
+                strat_group_epoch(g, epoch);
+            } catch (...) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                throw;
+            }
+            TSVD_CUDA(cudaEventRecord(e1, g->stream));
+            TSVD_CUDA(cudaStreamSynchronize(g->stream));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            g->last_epoch_ms = ms;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            g->epochs_run++;
+            return;
+        }
+        build_units(g, epoch);
+        upload_tables(g);
         TSVD_CUDA(cudaEventRecord(e0, g->stream));
         // The first epoch runs uncaptured (it also sets the kernels' launch
         // attributes); later epochs replay one captured graph.
@@ -297,6 +441,10 @@ int tsvd_group_autotune(tsvd_group* g, uint32_t sample_users, int32_t* chosen_st
     std::lock_guard<std::mutex> lk(g->mu);
     return gguard(g, [&] {
         TSVD_CUDA(cudaSetDevice(g->device));
+        if (g->stratified) {
+            strat_autotune(g, chosen_stages);
+            return;
+        }
         tsvd_model* m0 = g->models[0];
         const uint32_t U = m0->d.n_users;
         std::vector<uint32_t> users(U);

@@ -223,17 +223,19 @@ class TxModel:
 
 class TxGroup:
     """Several TxModel variants over one device copy of the data, trained
-    together: one persistent launch per epoch (a CUDA graph from the second
-    epoch on). `models[k]` is the Regressor view of variant k."""
+    together: stratified variants (the default) run their epochs on parallel
+    streams, Hogwild variants in one persistent launch per epoch; either way
+    an epoch of all variants is one CUDA graph from the second epoch on.
+    `models[k]` is the Regressor view of variant k."""
 
-    def __init__(self, tr: Dataset, pr, cfgs, device: int = 0):
+    def __init__(self, tr: Dataset, pr, cfgs, device: int = 0, schedule: int = SCHED_STRATIFIED):
         L = load()
         self._L = L
         self.cfgs = list(cfgs)
         n = len(self.cfgs)
         arr = (TsvdConfig * n)(*[c.to_c() for c in self.cfgs])
         opts = TsvdGpuOptions()
-        opts.schedule = SCHED_HOGWILD
+        opts.schedule = schedule
         opts.nsvd_norm_exp = 1.0
         opts.device = device
         tv = tr.view()
@@ -265,6 +267,8 @@ class TxGroup:
         return out.value
 
     def autotune(self, sample_users: int = 2000):
+        """Hogwild variants: the prefetch depth chosen per variant; stratified
+        variants: the item stratum's whole-CTA threshold per variant."""
         out = np.zeros(len(self.cfgs), np.int32)
         self._check(self._L.tsvd_group_autotune(self.h, sample_users, _p(out)))
         return out

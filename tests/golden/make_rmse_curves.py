@@ -10,7 +10,7 @@ generated arrays is stored beside the curve) and compare their own per-epoch
 RMSE with it.
 
 Cases (all with the tsvdx4 `lm` preset, src/bin/tsvdx4-new.rs:130-154, T=30):
-  c1        10,000 users x 2,000 items, 1,000,000 ratings, f=32, 20 epochs
+  c1_f32    10,000 users x 2,000 items, 1,000,000 ratings, f=32, 20 epochs
   c2_f64    480,189 x 17,770, 100,480,507 ratings, f=64, 40 epochs
   c2_f256   the same data, f=256, 60 epochs
 
@@ -18,7 +18,7 @@ The full-shape cases take hours on one core (the reference's epoch is
 single-threaded). The output file is rewritten after every epoch, so a run
 that stops early leaves the epochs it finished.
 
-  python tests/golden/make_rmse_curves.py --case c1
+  python tests/golden/make_rmse_curves.py --case c1_f32
 """
 from __future__ import annotations
 
@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 
 CASES = {
     # name: (spec function name, n_feat, epochs)
-    "c1": ("spec_c1", 32, 20),
+    "c1_f32": ("spec_c1", 32, 20),
     "c2_f64": ("spec_c2", 64, 40),
     "c2_f256": ("spec_c2", 256, 60),
 }

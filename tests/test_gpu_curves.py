@@ -69,7 +69,7 @@ def _run_curve(case, **model_kw):
 def test_c1_curve_tracks_reference_every_epoch():
     """C1 as written: 10,000 users x 2,000 items, 1,000,000 ratings, f=32,
     20 epochs, T=30."""
-    rows, worst = _run_curve("c1")
+    rows, worst = _run_curve("c1_f32")
     assert worst <= TOL, rows
 
 

@@ -10,6 +10,7 @@ graph. On shared-item data each variant's held-out RMSE must stay within
 import numpy as np
 import pytest
 
+from netflix_prize_b200.abi import SCHED_HOGWILD, SCHED_STRATIFIED
 from netflix_prize_b200.config import run_lm
 from netflix_prize_b200.data import MaskedDataset
 from netflix_prize_b200.model import TxGroup
@@ -31,7 +32,7 @@ def variants():
 def test_group_variants_equal_sequential_reference_without_races(graphs):
     tr, pr = disjoint_sets()
     cfgs = variants()
-    g = TxGroup(tr, MaskedDataset(pr), cfgs)
+    g = TxGroup(tr, MaskedDataset(pr), cfgs, schedule=SCHED_HOGWILD)
     g.set_graphs(graphs)
     oracles = [po.OracleModel(tr, MaskedDataset(pr), c) for c in cfgs]
     for e in (1, 2, 3):
@@ -51,7 +52,7 @@ def test_group_heldout_rmse_matches_each_sequential_variant():
     from tests.conftest import small_sets
     tr, pr = small_sets(n_users=4000, n_items=1000, n_train=400000, seed=3)
     cfgs = [c.replace(n_epochs=8) for c in variants()[:3]]
-    g = TxGroup(tr, MaskedDataset(pr), cfgs)
+    g = TxGroup(tr, MaskedDataset(pr), cfgs, schedule=SCHED_HOGWILD)
     oracles = [po.OracleModel(tr, MaskedDataset(pr), c) for c in cfgs]
     for e in range(1, 9):
         g.fit_epoch(e)
@@ -66,7 +67,7 @@ def test_group_heldout_rmse_matches_each_sequential_variant():
 def test_group_autotune_picks_a_depth_per_width_and_keeps_training_exact():
     tr, pr = disjoint_sets()
     cfgs = variants()
-    g = TxGroup(tr, MaskedDataset(pr), cfgs)
+    g = TxGroup(tr, MaskedDataset(pr), cfgs, schedule=SCHED_HOGWILD)
     before = [m.get_param("ifeat").copy() for m in g.models]
     stages = g.autotune(sample_users=32)
     assert all(s in (2, 3, 4) for s in stages)
@@ -77,3 +78,49 @@ def test_group_autotune_picks_a_depth_per_width_and_keeps_training_exact():
     o.fit_epoch(1, po.SCHED_SEQ)
     a = np.asarray(g.models[3].get_param("ufeat"), np.float64).ravel()
     assert np.max(np.abs(a - np.asarray(o.get_param("ufeat")))) < 2e-5
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_stratified_group_variants_equal_their_single_models(graphs):
+    """Stratified variants trained together (parallel streams, one captured
+    graph per epoch from the second on) equal, bit for bit, the same variants
+    trained one at a time: the schedule is deterministic."""
+    from netflix_prize_b200.model import TxModel
+    from tests.conftest import small_sets
+    tr, pr = small_sets(n_users=3000, n_items=80, n_train=90000, seed=13)
+    cfgs = [c.replace(reset_u_epoch=3, n_epochs=4) for c in variants()]
+    g = TxGroup(tr, MaskedDataset(pr), cfgs, schedule=SCHED_STRATIFIED)
+    g.set_graphs(graphs)
+    singles = [TxModel(tr, MaskedDataset(pr), c, heavy_item_ratings=0) for c in cfgs]
+    for e in (1, 2, 3, 4):
+        g.fit_epoch(e)
+        for m in singles:
+            m.fit_epoch(tr, pr, e)
+    for k, (gm, sm) in enumerate(zip(g.models, singles)):
+        for n in PARAMS + ["ycache", "ycache_bias"]:
+            a = np.asarray(gm.get_param(n), np.float32)
+            b = np.asarray(sm.get_param(n), np.float32)
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (k, n)
+    assert g.last_epoch_ms() > 0
+
+
+def test_stratified_group_autotune_picks_thresholds_and_keeps_results():
+    """The autotuner picks each variant's whole-CTA threshold on throwaway
+    copies; the group's own parameters are untouched and training still
+    follows the oracle's Tsvdx4pModel epoch."""
+    from tests.conftest import small_sets
+    tr, pr = small_sets(n_users=3000, n_items=80, n_train=90000, seed=13)
+    cfgs = variants()
+    g = TxGroup(tr, MaskedDataset(pr), cfgs, schedule=SCHED_STRATIFIED)
+    before = [m.get_param("ifeat").copy() for m in g.models]
+    thr = g.autotune()
+    assert all(t in (0x7fffffff, 65536, 32768, 16384, 8192, 4096) for t in thr)
+    for m, b in zip(g.models, before):
+        assert np.array_equal(m.get_param("ifeat"), b)
+    o = po.OracleModel(tr, MaskedDataset(pr), cfgs[2])
+    g.fit_epoch(1)
+    o.fit_epoch(1, po.SCHED_P, nsvd_norm_exp=1.0, n_threads=1)
+    for n in PARAMS:
+        a = np.asarray(g.models[2].get_param(n), np.float64).ravel()
+        b = np.asarray(o.get_param(n), np.float64).ravel()
+        assert np.max(np.abs(a - b) - 1e-5 * np.abs(b)) < 2e-5, n

@@ -165,6 +165,75 @@ __device__ __forceinline__ void tc_stage(const __nv_bfloat16* X, int x_km, int l
     }
 }
 
+// Register staging of one (ROWS x TC_K) operand tile: tc_load issues every
+// 16-byte global load of the tile at once (so their latencies overlap each
+// other and the tensor core's work on the previous block), tc_store writes
+// them into the core-matrix layout. Requires 16-byte aligned rows (`vec` in
+// tc_stage); element-wise fallbacks stay in tc_stage.
+template <int ROWS>
+struct TileRegs {
+    static constexpr int N = ROWS * TC_K / 8 / 128;  // 16-byte chunks per thread
+    uint4 v[N];
+};
+
+template <int ROWS>
+__device__ __forceinline__ void tc_load(const __nv_bfloat16* X, int x_km, int ld, int rows, int K, int r0, int k0,
+                                        TileRegs<ROWS>& t, int tid) {
+#pragma unroll
+    for (int c = 0; c < TileRegs<ROWS>::N; ++c) {
+        const int e = tid + 128 * c;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (!x_km) {
+            // 8 consecutive k of one row
+            const int r = e / (TC_K / 8), k8 = (e % (TC_K / 8)) * 8;
+            const int gr = r0 + r, gk = k0 + k8;
+            if (gr < rows) {
+                if (gk + 8 <= K) {
+                    v = __ldg(reinterpret_cast<const uint4*>(X + (size_t)gr * ld + gk));
+                } else {
+                    __nv_bfloat16 tt[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) tt[q] = gk + q < K ? X[(size_t)gr * ld + gk + q] : __float2bfloat16(0.0f);
+                    v = *reinterpret_cast<const uint4*>(tt);
+                }
+            }
+        } else {
+            // 8 consecutive rows at one k
+            const int r8 = (e % (ROWS / 8)) * 8, k = e / (ROWS / 8);
+            const int gr = r0 + r8, gk = k0 + k;
+            if (gk < K) {
+                if (gr + 8 <= rows) {
+                    v = __ldg(reinterpret_cast<const uint4*>(X + (size_t)gk * ld + gr));
+                } else {
+                    __nv_bfloat16 tt[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        tt[q] = gr + q < rows ? X[(size_t)gk * ld + gr + q] : __float2bfloat16(0.0f);
+                    v = *reinterpret_cast<const uint4*>(tt);
+                }
+            }
+        }
+        t.v[c] = v;
+    }
+}
+
+template <int ROWS>
+__device__ __forceinline__ void tc_store(int x_km, const TileRegs<ROWS>& t, uint8_t* tile, int tid) {
+#pragma unroll
+    for (int c = 0; c < TileRegs<ROWS>::N; ++c) {
+        const int e = tid + 128 * c;
+        if (!x_km) {
+            const int r = e / (TC_K / 8), k8 = (e % (TC_K / 8)) * 8;
+            *reinterpret_cast<uint4*>(tile + tc_off(r, k8)) = t.v[c];
+        } else {
+            const int r8 = (e % (ROWS / 8)) * 8, k = e / (ROWS / 8);
+            const __nv_bfloat16* tt = reinterpret_cast<const __nv_bfloat16*>(&t.v[c]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(r8 + q, k)) = tt[q];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restrict__ err) {
     extern __shared__ __align__(16) uint8_t tsm[];
     uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 2 * kTcStage);
@@ -189,8 +258,22 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
     const int kb0 = (int)blockIdx.z * per;
     const int nk = min(nk_all, kb0 + per) - kb0;
     float* const out_f32 = g.out_f32 ? g.out_f32 + (size_t)blockIdx.z * g.M * g.ldc : nullptr;
-    tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, kb0 * TC_K, tsm, tid);
-    tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, kb0 * TC_K, tsm + kTcABytes, tid);
+    // 16-byte rows on both operands: register-staged pipeline (the next
+    // block's loads in flight during this block's MMAs); else element-wise
+    const bool vec_a = (g.lda & 7) == 0 && (reinterpret_cast<uintptr_t>(g.A) & 15) == 0;
+    const bool vec_b = (g.ldb & 7) == 0 && (reinterpret_cast<uintptr_t>(g.B) & 15) == 0;
+    const bool piped = vec_a && vec_b;
+    TileRegs<TC_M> ra;
+    TileRegs<TC_N> rb;
+    if (piped) {
+        tc_load<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, kb0 * TC_K, ra, tid);
+        tc_load<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, kb0 * TC_K, rb, tid);
+        tc_store<TC_M>(g.a_km, ra, tsm, tid);
+        tc_store<TC_N>(g.b_kn, rb, tsm + kTcABytes, tid);
+    } else {
+        tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, kb0 * TC_K, tsm, tid);
+        tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, kb0 * TC_K, tsm + kTcABytes, tid);
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -216,6 +299,11 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
                          : "memory");
         }
         if (kb + 1 < nk) {
+            if (piped) {
+                // the next block's loads go out before the wait for the other stage
+                tc_load<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, (kb0 + kb + 1) * TC_K, ra, tid);
+                tc_load<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, (kb0 + kb + 1) * TC_K, rb, tid);
+            }
             // the other stage was read by block kb - 1's MMAs
             if (kb >= 1) {
                 const uint32_t ps = (uint32_t)((kb - 1) & 1), par = (uint32_t)(((kb - 1) >> 1) & 1);
@@ -224,8 +312,13 @@ __global__ void __launch_bounds__(128) k_gemm_tc(GemmArgs g, unsigned* __restric
                 asm volatile("tcgen05.fence::after_thread_sync;");
             }
             uint8_t* nxt = tsm + (st ^ 1u) * kTcStage;
-            tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, (kb0 + kb + 1) * TC_K, nxt, tid);
-            tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, (kb0 + kb + 1) * TC_K, nxt + kTcABytes, tid);
+            if (piped) {
+                tc_store<TC_M>(g.a_km, ra, nxt, tid);
+                tc_store<TC_N>(g.b_kn, rb, nxt + kTcABytes, tid);
+            } else {
+                tc_stage<TC_M>(g.A, g.a_km, g.lda, g.M, g.K, m0, (kb0 + kb + 1) * TC_K, nxt, tid);
+                tc_stage<TC_N>(g.B, g.b_kn, g.ldb, g.N, g.K, n0, (kb0 + kb + 1) * TC_K, nxt + kTcABytes, tid);
+            }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncthreads();

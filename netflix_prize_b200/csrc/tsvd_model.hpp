@@ -121,6 +121,8 @@ struct DeviceState {
     float* e_user;   // [U]     per-user error sum / norm
     float* pyc;      // [U, Fs] p_u + ycache_u for the item stratum; shares g_user's memory,
                      //         which the delta sums have consumed by then
+    float* qe0;      // [I, Fs] q_i + q^f_{i,0}, made before each user stratum (low_memory trains
+                     //         frequency bin 0, so the user stratum reads only this sum)
     unsigned long long* dyd_fix;  // [I, Fs] low_memory = false: the epoch's yfeat_day deltas,
                                   //         fixed point (kDydScale), added in any order
     // work lists
@@ -166,7 +168,7 @@ struct tsvd_model {
     tsvd::DevMem m_ubias, m_ibias, m_ufeat, m_ufeat2, m_ifeat, m_yfeat, m_ycache, m_yfeat_day;
     tsvd::DevMem m_alpha_u, m_but_bin, m_bit_bin, m_ybias, m_ycache_bias;
     tsvd::DevMem m_ubias_day, m_ufeat_day, m_ycache_day, m_ibias_freq, m_ifeat_freq, m_cu, m_cut, m_thresholds;
-    tsvd::DevMem m_dyd_fix;
+    tsvd::DevMem m_dyd_fix, m_qe0;
     tsvd::DevMem m_g_user, m_e_user, m_user_work, m_item_work, m_counters;
     // BF16 read copies (precision form)
     tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_pyc, m_bf_ufeat2;

@@ -517,6 +517,7 @@ void setup_params(tsvd_model* m) {
         zeros(m->m_cut, s.n_ud * 4, st);
         zeros(m->m_thresholds, 16, st);
         zeros(m->m_g_user, (size_t)U * Fs * 4, st);
+        if (c.low_memory) zeros(m->m_qe0, (size_t)I * Fs * 4, st);
         zeros(m->m_e_user, U * 4, st);
         zeros(m->m_counters, 64, st);
         m->m_perm.alloc(U * 4);
@@ -540,6 +541,7 @@ void setup_params(tsvd_model* m) {
         s.ufeat_day = c.low_memory ? nullptr : m->m_ufeat_day.as<float>();
         s.ycache_day = c.low_memory ? nullptr : m->m_ycache_day.as<float>();
         s.dyd_fix = c.low_memory ? nullptr : m->m_dyd_fix.as<unsigned long long>();
+        s.qe0 = c.low_memory ? m->m_qe0.as<float>() : nullptr;
         s.ibias_freq = m->m_ibias_freq.as<float>(); s.ifeat_freq = m->m_ifeat_freq.as<float>();
         s.cu = m->m_cu.as<float>(); s.cut = m->m_cut.as<float>();
         s.thresholds = m->m_thresholds.as<float>();

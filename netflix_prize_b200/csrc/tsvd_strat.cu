@@ -41,6 +41,19 @@ __global__ void k_to_bf16(const float* __restrict__ src, uint64_t rows, uint32_t
 }
 
 // The item rows a user-stratum rating reads: q_i and q^f_i of frequency bin fb.
+// qe0 = q_i + q^f_{i,0}: with low_memory the user stratum trains frequency bin
+// 0 only (src/tsvdx4p.rs:504-531) and reads the two rows only as this sum.
+__global__ void k_make_qe0(const float* __restrict__ ifeat, const float* __restrict__ ifeat_freq, uint64_t rows,
+                           uint32_t Fs, uint32_t NF, float* __restrict__ qe0) {
+    const uint64_t n = rows * Fs;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = e / Fs, c = e - r * Fs;
+        qe0[e] = ifeat[e] + ifeat_freq[r * NF * Fs + c];
+    }
+}
+
+void make_qe0(tsvd_model* m);
+
 template <int VPL, bool BF>
 __device__ __forceinline__ void item_rows(const DeviceState& s, const Bf16Copies& bf, uint32_t i, uint32_t fb, int lane,
                                           float (&q)[VPL], float (&qf)[VPL]) {
@@ -118,6 +131,8 @@ __device__ __forceinline__ void dyd_add(unsigned long long* row, int lane, const
 template <int VPL, bool BF, bool DAY>
 __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochParams p, Bf16Copies bf,
                                                          const uint32_t* __restrict__ order, uint32_t n_work) {
+    // FP32 with low_memory: the rating's item rows are read as their sum qe0
+    constexpr bool QE = !BF && !DAY;
     const int lane = threadIdx.x & 31;
     const uint32_t Fs = s.Fs, T = s.T, NF = s.NF;
     float th[4];
@@ -177,11 +192,12 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
             const uint32_t cnt = (uint32_t)(end - base < 32 ? end - base : 32);
             Rec mine{};
             if (lane < (int)cnt) mine = load_rec(s.rec + base + lane);
-            float qn[VPL], qfn[VPL];
-            {
-                const uint32_t k0 = __shfl_sync(kFull, mine.key, 0);
-                item_rows<VPL, BF>(s, bf, rec_id(k0), DAY ? rec_fbin(k0) : 0u, lane, qn, qfn);
-            }
+            float qn[VPL], qfn[QE ? 1 : VPL];
+            auto fetch_item = [&](uint32_t key) {
+                if constexpr (QE) Row<VPL>::load_nc(s.qe0 + (size_t)rec_id(key) * Fs, lane, qn);
+                else item_rows<VPL, BF>(s, bf, rec_id(key), DAY ? rec_fbin(key) : 0u, lane, qn, qfn);
+            };
+            fetch_item(__shfl_sync(kFull, mine.key, 0));
             for (uint32_t j = 0; j < cnt; ++j) {
                 const Rec r = shfl_rec(mine, j);
                 const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
@@ -219,16 +235,13 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
                             for (int v = 0; v < VPL; ++v) pud[v] = 0.0f;
                     }
                 }
-                float q[VPL], qf[VPL];
+                float qe[VPL];  // q_i + q^f_{i,fb}
 #pragma unroll
                 for (int v = 0; v < VPL; ++v) {
-                    q[v] = qn[v];
-                    qf[v] = qfn[v];
+                    if constexpr (QE) qe[v] = qn[v];
+                    else qe[v] = qn[v] + qfn[v];
                 }
-                if (j + 1 < cnt) {
-                    const uint32_t k1 = __shfl_sync(kFull, mine.key, j + 1);
-                    item_rows<VPL, BF>(s, bf, rec_id(k1), DAY ? rec_fbin(k1) : 0u, lane, qn, qfn);
-                }
+                if (j + 1 < cnt) fetch_item(__shfl_sync(kFull, mine.key, j + 1));
                 const float ib = __ldg(s.ibias + i);
                 const float bit = __ldg(s.bit_bin + (size_t)i * T + tb);
                 const float ibf = __ldg(s.ibias_freq + (size_t)i * NF + fb);
@@ -249,7 +262,7 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
                         if (p.has_ud && hud) pev += pud[v];
                         pev += sud[v];
                     }
-                    part += (q[v] + qf[v]) * pev;
+                    part += qe[v] * pev;
                 }
                 const float dot = warp_sum(part);
                 const float err = rating_err(s, th, gb + bu_t + bi_t * cu_t + dot, r.res);
@@ -267,14 +280,13 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
                 sum_err += err;
 #pragma unroll
                 for (int v = 0; v < VPL; ++v) {
-                    const float qe = q[v] + qf[v];
                     const float pk = pu[v], p2k = p2[v];
-                    seq[v] += err * qe;
-                    pu[v] = pk - p.lr_u * (err * qe + p.reg_u * pk);
-                    p2[v] = p2k - p.lr_u2 * (err * qe * dv + p.reg_u2 * p2k);
+                    seq[v] += err * qe[v];
+                    pu[v] = pk - p.lr_u * (err * qe[v] + p.reg_u * pk);
+                    p2[v] = p2k - p.lr_u2 * (err * qe[v] * dv + p.reg_u2 * p2k);
                     if constexpr (DAY) {
-                        seqd[v] += err * qe;
-                        if (p.has_ud && hud) pud[v] = pud[v] - p.lr_ud * (err * qe + p.reg_ud * pud[v]);
+                        seqd[v] += err * qe[v];
+                        if (p.has_ud && hud) pud[v] = pud[v] - p.lr_ud * (err * qe[v] + p.reg_ud * pud[v]);
                     }
                 }
                 if constexpr (DAY) {
@@ -1295,8 +1307,7 @@ __global__ void __launch_bounds__(kThreads) k_user_strat_wide(DeviceState s, Epo
                 const Rec r = shfl_rec(mine, j);
                 const uint32_t i = rec_id(r.key), tb = rec_tbin(r.key);
                 const bool hud = r.ud < s.n_ud;
-                const float* q_row = s.ifeat + (size_t)i * Fs;
-                const float* qf_row = s.ifeat_freq + (size_t)i * NF * Fs;  // low_memory: bin 0
+                const float* qe_row = s.qe0 + (size_t)i * Fs;  // q_i + q^f_{i,0} (low_memory: bin 0)
                 const float ib = __ldg(s.ibias + i);
                 const float bit = __ldg(s.bit_bin + (size_t)i * T + tb);
                 const float ibf = __ldg(s.ibias_freq + (size_t)i * NF);
@@ -1311,14 +1322,13 @@ __global__ void __launch_bounds__(kThreads) k_user_strat_wide(DeviceState s, Epo
                 const float cu_t = cuu + ct;
                 float part = 0.0f;
                 for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
-                    float q[kWV], qf[kWV], pu[kWV], su[kWV], p2[kWV];
-                    R8::load_nc(q_row + c0, lane, q);
-                    R8::load_nc(qf_row + c0, lane, qf);
+                    float qe[kWV], pu[kWV], su[kWV], p2[kWV];
+                    R8::load_nc(qe_row + c0, lane, qe);
                     R8::load_cg(pu_row + c0, lane, pu);
                     R8::load_cg(su_row + c0, lane, su);
                     R8::load_cg(p2_row + c0, lane, p2);
 #pragma unroll
-                    for (int v = 0; v < kWV; ++v) part += (q[v] + qf[v]) * ((pu[v] + su[v]) + dv * p2[v]);
+                    for (int v = 0; v < kWV; ++v) part += qe[v] * ((pu[v] + su[v]) + dv * p2[v]);
                 }
                 const float dot = warp_sum(part);
                 const float err = rating_err(s, th, gb + bu_t + bi_t * cu_t + dot, r.res);
@@ -1335,15 +1345,14 @@ __global__ void __launch_bounds__(kThreads) k_user_strat_wide(DeviceState s, Epo
                 cuu -= p.lr_cu * (err * bi_t + p.reg_cu * (cuu - 1.0f));
                 sum_err += err;
                 for (uint32_t c0 = 0; c0 < Fs; c0 += kSlice) {
-                    float q[kWV], qf[kWV], pu[kWV], p2[kWV], sq[kWV];
-                    R8::load_nc(q_row + c0, lane, q);
-                    R8::load_nc(qf_row + c0, lane, qf);
+                    float qev[kWV], pu[kWV], p2[kWV], sq[kWV];
+                    R8::load_nc(qe_row + c0, lane, qev);
                     R8::load_cg(pu_row + c0, lane, pu);
                     R8::load_cg(p2_row + c0, lane, p2);
                     R8::load_cg(sq_row + c0, lane, sq);
 #pragma unroll
                     for (int v = 0; v < kWV; ++v) {
-                        const float qe = q[v] + qf[v];
+                        const float qe = qev[v];
                         const float pk = pu[v], p2k = p2[v];
                         sq[v] += err * qe;
                         pu[v] = pk - p.lr_u * (err * qe + p.reg_u * pk);
@@ -1459,6 +1468,7 @@ __global__ void __launch_bounds__(kThreads) k_item_wide(DeviceState s, EpochPara
 
 void strat_launch_wide(tsvd_model* m, const EpochParams& p) {
     const DeviceState& s = m->d;
+    make_qe0(m);
     {
         ProfScope ps(m, "user_pass_stratified");
         unsigned g = persistent_grid(k_user_strat_wide, 0);
@@ -1484,6 +1494,15 @@ void strat_launch_wide(tsvd_model* m, const EpochParams& p) {
     }
 }
 
+void make_qe0(tsvd_model* m) {
+    const DeviceState& s = m->d;
+    if (!s.qe0) return;
+    const unsigned grid = (unsigned)std::min<uint64_t>(((uint64_t)s.n_items * s.Fs + 255) / 256, 148ull * 32);
+    k_make_qe0<<<grid, 256, 0, m->stream>>>(s.ifeat, s.ifeat_freq, s.n_items, s.Fs, s.NF, s.qe0);
+    TSVD_CUDA(cudaGetLastError());
+    m->launches++;
+}
+
 void to_bf16(tsvd_model* m, const float* src, uint64_t rows, uint64_t src_stride, void* dst) {
     const uint32_t Fs = m->d.Fs;
     const unsigned grid = (unsigned)std::min<uint64_t>((rows * Fs + 255) / 256, 148ull * 32);
@@ -1503,6 +1522,7 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     DeviceState s = m->d;
     if (DAY || s.raw) s.heavy_min = 0xffffffffu;
     if (DAY) TSVD_CUDA(cudaMemsetAsync(s.dyd_fix, 0, (size_t)s.n_items * s.Fs * 8, m->stream));
+    if (!BF && !DAY) make_qe0(m);
     {
         ProfScope ps(m, "user_pass_stratified");
         unsigned g = persistent_grid(k_user_strat<VPL, BF, DAY>, 0);
@@ -1566,6 +1586,7 @@ __global__ void k_reset_users(DeviceState s, const uint32_t* __restrict__ users,
 // which the next stratified epoch clears before its user stratum.)
 template <int VPL>
 void foldin_launch(tsvd_model* m, const EpochParams& p, const uint32_t* d_users, uint32_t n) {
+    make_qe0(m);
     if (m->d.dyd_fix) {
         unsigned g = persistent_grid(k_user_strat<VPL, false, true>, 0);
         k_user_strat<VPL, false, true><<<g, kThreads, 0, m->stream>>>(m->d, p, Bf16Copies{}, d_users, n);
@@ -1587,6 +1608,7 @@ template <int VPL, bool DAY>
 void shard_user_launch(tsvd_model* m, const EpochParams& p, const uint32_t* work, uint32_t n, uint32_t u_lo,
                        uint32_t u_hi, float* sums, float* sums_e) {
     const DeviceState& s = m->d;
+    if (!DAY) make_qe0(m);
     {
         ProfScope ps(m, "user_pass_stratified");
         if (s.Fs > kSlice) {

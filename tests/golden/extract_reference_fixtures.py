@@ -6,14 +6,17 @@ Reads (text only, nothing is executed):
   tests/regressors_test.rs:28-73  the shared regression-test config
   tests/regressors_test.rs:75-93  tsvdx4 probe RMSE known answer
   tests/regressors_test.rs:157-175 tsvdx4p probe RMSE known answer
-Run from the repo root:  python tests/golden/extract_reference_fixtures.py [REF_ROOT]
+Run from the repo root:  python tests/golden/extract_reference_fixtures.py REF_ROOT
+(REF_ROOT: a checkout of the reference repository).
 """
 import json
 import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: extract_reference_fixtures.py REF_ROOT")
+ref = sys.argv[1]
 helpers = open(os.path.join(ref, "tests/helpers.rs")).read()
 regs = open(os.path.join(ref, "tests/regressors_test.rs")).read()
 

@@ -54,6 +54,7 @@ __global__ void k_make_qe0(const float* __restrict__ ifeat, const float* __restr
 
 void make_qe0(tsvd_model* m);
 
+
 template <int VPL, bool BF>
 __device__ __forceinline__ void item_rows(const DeviceState& s, const Bf16Copies& bf, uint32_t i, uint32_t fb, int lane,
                                           float (&q)[VPL], float (&qf)[VPL]) {
@@ -326,11 +327,15 @@ __global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochPar
 // (k_y_partial), then each item adds its chunk partials in chunk order and
 // applies the update (k_y_combine).
 // ---------------------------------------------------------------------------
-// Entries whose user lies outside [u_lo, u_hi) are left out (a sharded run's
-// user block; the full range otherwise). An item's entries are sorted by user,
-// so the ones kept are contiguous and keep their order.
+// Entries whose user lies outside [u_lo, u_hi) are left out (a user block; the
+// full range otherwise). An item's entries are sorted by user, so the ones
+// kept are contiguous and keep their order. With `accumulate` the block's
+// partial is added to the chunk's earlier blocks' (blocks in user order), and
+// chunks without entries in the block are left alone: passes over user blocks
+// whose g_user rows fit in L2 gather from L2 instead of HBM.
 template <int VPL>
-__global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t u_lo, uint32_t u_hi) {
+__global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t u_lo, uint32_t u_hi,
+                                                        int accumulate) {
     const int lane = threadIdx.x & 31;
     const uint32_t Fs = s.Fs;
     constexpr int B = 8;  // rows in flight per warp
@@ -358,6 +363,7 @@ __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t 
             }
             a = lo;
             b = lo2;
+            if (accumulate && a == b) continue;
         }
         // rows wider than 32 * VPL columns (n_feat > 256) in slices
         for (uint32_t c0 = 0; c0 < Fs; c0 += 32 * VPL) {
@@ -386,9 +392,36 @@ __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t 
                     }
                 }
             }
+            if (accumulate) {
+                float prev[VPL];
+                Row<VPL>::load_cg(s.chunk_part + (size_t)c * Fs + c0, lane, prev);
+#pragma unroll
+                for (int v = 0; v < VPL; ++v) acc[v] = prev[v] + acc[v];
+                if (c0 == 0) eacc = __ldcg(s.chunk_epart + c) + eacc;
+            }
             Row<VPL>::store(s.chunk_part + (size_t)c * Fs + c0, lane, acc);
             if (lane == 0 && c0 == 0) s.chunk_epart[c] = eacc;
         }
+    }
+}
+
+// The NSVD1 delta sums of users u_lo..u_hi-1 into the chunk partials, in
+// passes over user blocks of at most ~64 MB of g_user rows (L2 holds one).
+template <int VPL>
+void y_partial_passes(tsvd_model* m, const DeviceState& s, uint32_t u_lo, uint32_t u_hi) {
+    const uint64_t row_bytes = (uint64_t)s.Fs * 4;
+    const uint32_t per = (uint32_t)std::max<uint64_t>(1, (64ull << 20) / row_bytes);
+    const unsigned g = persistent_grid(k_y_partial<VPL>, 0);
+    const bool whole = u_lo == 0 && u_hi >= s.n_users;
+    for (uint64_t b0 = u_lo; b0 < u_hi || b0 == u_lo; b0 += per) {
+        const uint32_t b1 = (uint32_t)std::min<uint64_t>(u_hi, b0 + per);
+        TSVD_CUDA(cudaMemsetAsync(s.counters + 1, 0, 4, m->stream));
+        const bool one = whole && b1 >= u_hi && b0 == u_lo;  // a single pass over every user
+        k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, one ? 0u : (uint32_t)b0, one ? 0xffffffffu : b1,
+                                                        b0 == u_lo ? 0 : 1);
+        TSVD_CUDA(cudaGetLastError());
+        m->launches++;
+        if (b1 >= u_hi) break;
     }
 }
 
@@ -1478,11 +1511,10 @@ void strat_launch_wide(tsvd_model* m, const EpochParams& p) {
     }
     {
         ProfScope ps(m, "y_apply");
-        unsigned g = persistent_grid(k_y_partial<kWV>, 0);
-        k_y_partial<kWV><<<g, kThreads, 0, m->stream>>>(s, 0u, 0xffffffffu);
+        y_partial_passes<kWV>(m, s, 0, s.n_users);
         k_y_combine<kWV><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, p);
         TSVD_CUDA(cudaGetLastError());
-        m->launches += 2;
+        m->launches++;
     }
     launch_rebuild_ycache(m, s.pyc);
     {
@@ -1532,11 +1564,10 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     }
     {
         ProfScope ps(m, "y_apply");
-        unsigned g = persistent_grid(k_y_partial<VPL>, 0);
-        k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, 0u, 0xffffffffu);
+        y_partial_passes<VPL>(m, s, 0, s.n_users);
         k_y_combine<VPL><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, p);
         TSVD_CUDA(cudaGetLastError());
-        m->launches += 2;
+        m->launches++;
     }
     if (BF) to_bf16(m, s.yfeat, s.n_items, s.Fs, m->m_bf_yfeat.p);
     launch_rebuild_ycache(m, s.pyc);
@@ -1622,11 +1653,10 @@ void shard_user_launch(tsvd_model* m, const EpochParams& p, const uint32_t* work
         m->launches++;
     }
     ProfScope ps(m, "y_apply");
-    unsigned g = persistent_grid(k_y_partial<VPL>, 0);
-    k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, u_lo, u_hi);
+    y_partial_passes<VPL>(m, s, u_lo, u_hi);
     k_y_block_sums<VPL><<<ceil_div(s.n_items, kWarps), kThreads, 0, m->stream>>>(s, sums, sums_e);
     TSVD_CUDA(cudaGetLastError());
-    m->launches += 2;
+    m->launches++;
 }
 
 template <int VPL, bool DAY>

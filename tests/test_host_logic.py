@@ -65,3 +65,42 @@ def test_generator_is_seeded():
     a, _ = synth.generate(s)
     b, _ = synth.generate(s)
     assert np.array_equal(a.item_idxs, b.item_idxs) and np.array_equal(a.raw_ratings, b.raw_ratings)
+
+
+def test_job_table_covers_the_dispatchers_base_jobs():
+    """All 19 tsvdx4 base jobs (src/bin/tsvdx4-new.rs:18-40), spot-checked
+    against the presets (:118-556)."""
+    from netflix_prize_b200.jobs import JOBS
+    assert len(JOBS) == 19
+    assert JOBS["tsvdx4-4800lm"].config.n_feat == 4800 and JOBS["tsvdx4-4800lm"].config.n_epochs == 27
+    assert JOBS["tsvdx4-60"].config.low_memory is False and JOBS["tsvdx4-60"].save_train
+    assert JOBS["tsvdx4-d0tb"].config.n_feat == 0 and JOBS["tsvdx4-p0tbo"].config.ordinal_head is not None
+    assert JOBS["tsvdx4-q16tb"].config.n_time_bins == 48 and JOBS["tsvdx4-s20fo"].config.n_freq_bins == 24
+    assert JOBS["tsvdx4-16-t"].transpose and JOBS["tsvdx4-16-t"].config.beta == 0.35
+    assert JOBS["tsvdx4-80o"].save_subscores and not JOBS["tsvdx4-80o"].save_train
+    for name, job in JOBS.items():
+        c = job.config
+        assert c.lr_w == c.lr_c == c.lr_w_day == c.lr_c_day == 0.0, name   # tx4 mode
+        assert c.ordinal_head is None or c.ordinal_head.lr_t == 0.0, name
+
+
+def test_transpose_swaps_roles_and_orders_by_item_then_date():
+    """Dataset::transpose (src/lib.rs:295-405): with reorder, a stable order
+    by (old item, date); without, the rows keep their order."""
+    import numpy as np
+    from netflix_prize_b200.data import Dataset
+    rng = np.random.default_rng(3)
+    u = np.sort(rng.integers(0, 50, 400))
+    i = rng.integers(0, 30, 400)
+    d = rng.integers(0, 100, 400)
+    r = rng.integers(1, 6, 400)
+    ds = Dataset.from_ratings(u, i, r, d, 50, 30, "t")
+    t = ds.transpose(True)
+    assert (t.n_users, t.n_items) == (30, 50) and t.transposed
+    key = i.astype(np.int64) * 1000 + d
+    o = np.argsort(key, kind="stable")
+    assert np.array_equal(t.user_idxs, i[o]) and np.array_equal(t.item_idxs, u[o])
+    assert np.array_equal(t.dates, d[o]) and np.array_equal(t.raw_ratings, r[o])
+    assert np.array_equal(t.user_cnts, ds.item_cnts) and np.array_equal(t.item_cnts, ds.user_cnts)
+    s = ds.transpose(False)
+    assert np.array_equal(s.user_idxs, i) and np.array_equal(s.item_idxs, u)

@@ -215,7 +215,18 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         uoff[u + 1] = uoff[u] + (uint64_t)tr.user_cnts[u];
     }
     if (uoff[U] != R) throw Error(TSVD_ERR_INVALID, "training user_cnts do not sum to n_ratings");
-    {
+    // Every rating of user u lies in uoff[u] .. uoff[u+1] and its item is in
+    // range: checked over users in parallel; a failure reruns the checks in
+    // rating order for the reference's message.
+    bool rows_ok = true;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(&& : rows_ok)
+    for (int64_t uu = 0; uu < (int64_t)U; ++uu) {
+        for (uint64_t t = uoff[uu]; t < uoff[uu + 1]; ++t) {
+            const int32_t i = tr.item_idxs[t];
+            rows_ok = rows_ok && tr.user_idxs[t] == (int32_t)uu && i >= 0 && (uint32_t)i < I;
+        }
+    }
+    if (!rows_ok) {
         uint32_t prev = 0;
         for (uint64_t t = 0; t < R; ++t) {
             int32_t u = tr.user_idxs[t];
@@ -226,11 +237,9 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
             int32_t i = tr.item_idxs[t];
             if (i < 0 || (uint32_t)i >= I) throw Error(TSVD_ERR_INVALID, "training item index out of range");
         }
-        for (uint32_t u = 0; u < U; ++u) {
-            uint64_t e = uoff[u + 1];
-            if (e > uoff[u] && ((uint32_t)tr.user_idxs[uoff[u]] != u || (uint32_t)tr.user_idxs[e - 1] != u))
-                throw Error(TSVD_ERR_INVALID, "training user_cnts disagree with user_idxs");
-        }
+        throw Error(TSVD_ERR_INVALID, "training user_cnts disagree with user_idxs");
+    }
+    {
         std::vector<int64_t> pcnt(U, 0);
         for (uint64_t t = 0; t < P; ++t) {
             int32_t u = pr.user_idxs[t], i = pr.item_idxs[t];
@@ -241,17 +250,27 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         for (uint32_t u = 0; u < U; ++u)
             if (pcnt[u] != pr.user_cnts[u]) throw Error(TSVD_ERR_INVALID, "pr user_cnts disagree with user_idxs");
     }
-    // tu_mean in f32, summed in rating order; day_range; gbias (src/tx.rs:465-475, src/lib.rs:463-467)
+    // tu_mean in f32, summed in rating order; day_range; gbias (src/tx.rs:465-475,
+    // src/lib.rs:463-467). Users in parallel: a user's dates add in rating
+    // order, so tu_mean is the reference's; the FP64 residual sum adds the
+    // users' sums in user order (exact for integer residuals).
     std::vector<float> tum(U, 0.0f);
+    std::vector<double> usum(U, 0.0);
     int32_t dr = 0;
-    double rsum = 0.0;
-    for (uint64_t t = 0; t < R; ++t) {
-        tum[tr.user_idxs[t]] += (float)tr.dates[t];
-        dr = std::max(dr, (int32_t)tr.dates[t] + 1);
-        rsum += (double)tr.residuals[t];
+#pragma omp parallel for schedule(dynamic, 4096) reduction(max : dr)
+    for (int64_t uu = 0; uu < (int64_t)U; ++uu) {
+        float a = 0.0f;
+        double b = 0.0;
+        for (uint64_t t = uoff[uu]; t < uoff[uu + 1]; ++t) {
+            a += (float)tr.dates[t];
+            dr = std::max(dr, (int32_t)tr.dates[t] + 1);
+            b += (double)tr.residuals[t];
+        }
+        tum[uu] = tr.user_cnts[uu] > 0 ? a / (float)tr.user_cnts[uu] : a;
+        usum[uu] = b;
     }
-    for (uint32_t u = 0; u < U; ++u)
-        if (tr.user_cnts[u] > 0) tum[u] /= (float)tr.user_cnts[u];
+    double rsum = 0.0;
+    for (uint32_t u = 0; u < U; ++u) rsum += usum[u];
     if (dr <= 0) throw Error(TSVD_ERR_INVALID, "training dates must include a non-negative day");
 
     // Rows padded with zeros (which every update keeps at zero): to a multiple
@@ -424,7 +443,14 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         TSVD_CUDA(cudaGetLastError());
         std::vector<uint64_t> ioff(I + 1, 0);
         std::vector<uint32_t> icnt(I, 0);
-        for (uint64_t t = 0; t < R; ++t) icnt[tr.item_idxs[t]]++;
+#pragma omp parallel
+        {
+            std::vector<uint32_t> mine(I, 0);
+#pragma omp for schedule(static) nowait
+            for (int64_t t = 0; t < (int64_t)R; ++t) mine[tr.item_idxs[t]]++;
+#pragma omp critical
+            for (uint32_t i = 0; i < I; ++i) icnt[i] += mine[i];
+        }
         for (uint32_t i = 0; i < I; ++i) ioff[i + 1] = ioff[i] + icnt[i];
         upload(m->m_item_off, ioff.data(), I + 1, st);
         s.irec = m->m_irec.as<Rec>();

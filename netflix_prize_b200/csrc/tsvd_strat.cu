@@ -565,10 +565,8 @@ static_assert(kPW * 4 == kRound, "each producer warp stages four of the round's 
 
 // Shared-memory layout of the item pass, in floats (every offset a multiple of 4).
 struct ItemSmem {
-    uint32_t qfs, qsh, buf, hl, mbuf, vec, pd, sv, ap, st, pw, gp, od, total;
+    uint32_t qfs, qsh, buf, hl, mbuf, vec, pd, sv, ap, st, pw, total;
 };
-constexpr int kGW = 4;               // producer warps that form the round's Gram matrix
-constexpr uint32_t kGS = kRound + 1; // row stride of a Gram partial
 __host__ __device__ inline ItemSmem item_smem(uint32_t Fs, uint32_t NF) {
     ItemSmem L;
     uint32_t o = 0;
@@ -583,8 +581,6 @@ __host__ __device__ inline ItemSmem item_smem(uint32_t Fs, uint32_t NF) {
     L.ap = o;   o += 4 * kRound;                // per rating {w_q, w_f, decay, bin | previous << 8}
     L.st = o;   o += 132;                       // the item's biases: ib, bit_bin[64], ibias_freq[64]
     L.pw = o;   o += 2 * 36;                    // a_i^n, a_f^n for n = 0..kRound
-    L.gp = o;   o += kGW * kRound * kGS;        // the Gram warps' partial sums over their K ranges
-    L.od = o;   o += 2 * 2 * kRound;            // two rounds of the ratings ordered by q^f bin, by time bin
     L.total = o;
     return L;
 }
@@ -810,6 +806,7 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
     __shared__ uint32_t sh_k;
     static_assert(kCW == 4, "the consumers' partial dots are summed as (0 + 1) + (2 + 3)");
     constexpr int CPL = (VPL + kCW - 1) / kCW;  // 32-column stripes per consumer warp
+    constexpr int kChunk = 8;                   // ratings per step of the consumers' apply
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t Fs = s.Fs, NF = s.NF, T = s.T, NS = Fs / 32;
     const uint32_t stride = Fs + 4;  // one staged rating: pe row + {bu_t, cu_t, res, key}
@@ -828,8 +825,6 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
     float* sst = smem + L.st;
     float* apow = smem + L.pw;  // apow[n] = a_i^n, fpow[n] = a_f^n (products in order)
     float* fpow = apow + 36;
-    float* gp = smem + L.gp;
-    int* od = reinterpret_cast<int*>(smem + L.od);
     // update factors: x - lr (g + reg x) = a x - lr g
     const float a_i = 1.0f - p.lr_i * p.reg_i, a_f = 1.0f - p.lr_iqf * p.reg_iqf;
     if (threadIdx.x == 0) {
@@ -976,45 +971,64 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
             const uint32_t fbl = rec_fbin(mine.key);
             // the round's ratings of each frequency bin (valid ratings only)
             const unsigned same = __match_any_sync(kFull, valid ? fbl : 64u + (uint32_t)lane);
-            if (pw < kGW) {
-                // G = PE PE^T on the tensor cores from BF16 high and low parts
-                // of pe (three products: error ~2^-16 of |pe_i||pe_j|), over
-                // this warp's share of the K steps. The round's rows are read
-                // from shared memory once: the B operand of rows 8n..8n+7
-                // (k x 8) is two of the four 8x8 matrices of their A operand.
-                // Six 16x8 tiles hold every pair row < column.
+            if (pw < 6) {
+                // G = PE PE^T on the tensor cores, from BF16 high and low
+                // parts of pe (three products: error ~2^-16 of |pe_i||pe_j|).
+                // Tile pw of the six 16x8 tiles (rows x columns) that hold
+                // every pair row < column.
+                const int mt = pw < 4 ? 0 : 1, nt = pw < 4 ? pw : pw - 2;
                 const int gid = lane >> 2, tig = lane & 3;
+                // ldmatrix row addresses: A (16x16) as four 8x8 matrices
+                // (rows 0-7 | 8-15) x (k 0-7 | 8-15); B's high and low parts
+                // (8 pe rows x k 0-7 | 8-15) in one x4
                 const uint32_t hl_s = smem_u32(hl);
-                const int ar = (lane & 7) + 8 * ((lane >> 3) & 1), ak = 8 * (lane >> 4);
-                const uint32_t a0 = hl_s + (uint32_t)(ar * hp + 2 * ak);  // rows 0-15, high parts
-                const uint32_t a1 = a0 + (uint32_t)(16 * hp);              // rows 16-31
-                const uint32_t lo = (uint32_t)(kRound * hp);               // high -> low parts
-                const uint32_t nks = Fs / 16, k_lo = (uint32_t)pw * nks / kGW, k_hi = (uint32_t)(pw + 1) * nks / kGW;
-                float acc[6][4] = {};
-                for (uint32_t ks = k_lo; ks < k_hi; ++ks) {
-                    const uint32_t kb = 32u * ks;  // 16 BF16 per step
-                    uint32_t h0[4], h1[4], l0[4], l1[4];
-                    ldmatrix_x4(h0, a0 + kb);
-                    ldmatrix_x4(h1, a1 + kb);
-                    ldmatrix_x4(l0, a0 + lo + kb);
-                    ldmatrix_x4(l1, a1 + lo + kb);
-                    const uint32_t bh[4][2] = {{h0[0], h0[2]}, {h0[1], h0[3]}, {h1[0], h1[2]}, {h1[1], h1[3]}};
-                    const uint32_t bl[4][2] = {{l0[0], l0[2]}, {l0[1], l0[3]}, {l1[0], l1[2]}, {l1[1], l1[3]}};
+                const int ar = mt * 16 + (lane & 7) + 8 * ((lane >> 3) & 1), ak = 8 * (lane >> 4);
+                const uint32_t a_hi = hl_s + (uint32_t)(ar * hp + 2 * ak);
+                const uint32_t a_lo = a_hi + (uint32_t)(kRound * hp);
+                const int br = nt * 8 + (lane & 7), bk = 8 * ((lane >> 3) & 1);
+                const uint32_t b_hl = hl_s + (uint32_t)(((lane >> 4) * kRound + br) * hp + 2 * bk);
+                float d[6][4] = {};
+#pragma unroll 2
+                for (uint32_t k0 = 0; k0 < Fs; k0 += 32) {
 #pragma unroll
-                    for (int t = 0; t < 6; ++t) {
-                        const int nt = t < 4 ? t : t - 2;
-                        mma_bf16(acc[t], t < 4 ? l0 : l1, bh[nt]);  // the small cross terms first
-                        mma_bf16(acc[t], t < 4 ? h0 : h1, bl[nt]);
-                        mma_bf16(acc[t], t < 4 ? h0 : h1, bh[nt]);
+                    for (int hh = 0; hh < 2; ++hh) {
+                        const uint32_t kb = 2 * (k0 + 16 * hh);
+                        uint32_t ah[4], al[4], bb[4];
+                        ldmatrix_x4(ah, a_hi + kb);
+                        ldmatrix_x4(al, a_lo + kb);
+                        ldmatrix_x4(bb, b_hl + kb);
+                        const uint32_t bh[2] = {bb[0], bb[1]}, bl[2] = {bb[2], bb[3]};
+                        mma_bf16(d[3 * hh], al, bh);
+                        mma_bf16(d[3 * hh + 1], ah, bl);
+                        mma_bf16(d[3 * hh + 2], ah, bh);
                     }
                 }
-                float* G = gp + (size_t)pw * kRound * kGS;
+                // The round's errors solve err = C - M err with M unit lower
+                // triangular: M_ji (i < j) is the effect of err_i on rating j
+                // through q (a_i^(j-1-i) G_ij), the q^f row of a shared bin
+                // (a_f^(same-bin ratings between) G_ij) and the item biases.
+                // This lane's four entries (i, j) give M_ji and M_ij = 0.
 #pragma unroll
-                for (int t = 0; t < 6; ++t) {
-                    const int mt = t < 4 ? 0 : 1, nt = t < 4 ? t : t - 2;
-#pragma unroll
-                    for (int e = 0; e < 4; ++e)
-                        G[(mt * 16 + gid + 8 * (e >> 1)) * kGS + nt * 8 + 2 * tig + (e & 1)] = acc[t][e];
+                for (int e = 0; e < 4; ++e) {
+                    const float g = ((d[0][e] + d[1][e]) + (d[3][e] + d[4][e])) + (d[2][e] + d[5][e]);
+                    const int ii = mt * 16 + gid + 8 * (e >> 1), jj = nt * 8 + 2 * tig + (e & 1);
+                    const uint32_t ki = __shfl_sync(kFull, mine.key, ii), kj = __shfl_sync(kFull, mine.key, jj);
+                    const unsigned samej = __shfl_sync(kFull, same, jj);
+                    if (ii < jj) {
+                        float v = 0.0f;
+                        if (jj < (int)m) {
+                            const float cui = dst[(size_t)ii * stride + Fs + 1], cuj = dst[(size_t)jj * stride + Fs + 1];
+                            const bool same_f = rec_fbin(ki) == rec_fbin(kj), same_t = rec_tbin(ki) == rec_tbin(kj);
+                            const float bias_lr = p.lr_ib + (same_t ? p.lr_ti : 0.0f) + (same_f ? p.lr_ibf : 0.0f);
+                            const unsigned between = ((1u << jj) - 1u) & ~((2u << ii) - 1u);
+                            v = cuj * cui * bias_lr + p.lr_i * apow[jj - 1 - ii] * g +
+                                (same_f ? p.lr_iqf * fpow[__popc(samej & between)] * g : 0.0f);
+                        }
+                        Mb[(size_t)jj * kMS + ii] = v;
+                        Mb[(size_t)ii * kMS + jj] = 0.0f;
+                    } else if (ii == jj) {
+                        Mb[(size_t)ii * kMS + ii] = 0.0f;
+                    }
                 }
             } else if (pw == 6) {
                 // per-rating weights of the round (j = lane)
@@ -1026,57 +1040,11 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                 V[3 * kRound + lane] = fpow[__popc(same & above)];          // a_f^(later ratings of the bin)
                 // the first rating of a bin applies the decay of all its ratings to the bin's row
                 V[4 * kRound + lane] = (valid && earlier == 0u) ? fpow[__popc(same)] : 1.0f;
+                V[5 * kRound + lane] = __uint_as_float(fbl);
                 if (lane == 0) V[6 * kRound] = apow[m];                     // a_i^m
-            } else if (pw == 7) {
-                // The round's ratings in a stable order by q^f bin, and by
-                // time bin, ratings past m last: entry = j | first of its bin
-                // << 8 | last of its bin << 9 | past m << 10 | bin << 16.
-                int* OD = od + (size_t)(r & 1) * 2 * kRound;
-#pragma unroll
-                for (int w = 0; w < 2; ++w) {
-                    const uint32_t bin = w == 0 ? fbl : rec_tbin(mine.key);
-                    const uint32_t key = valid ? bin : 64u + (uint32_t)lane;
-                    uint32_t rank = 0;
-                    for (int i2 = 0; i2 < kRound; ++i2) {
-                        const uint32_t ki = __shfl_sync(kFull, key, i2);
-                        rank += (ki < key || (ki == key && i2 < lane)) ? 1u : 0u;
-                    }
-                    const unsigned grp = __match_any_sync(kFull, key);
-                    const uint32_t head = (uint32_t)(__ffs(grp) - 1) == (uint32_t)lane ? 1u : 0u;
-                    const uint32_t tail = (uint32_t)(31 - __clz(grp)) == (uint32_t)lane ? 1u : 0u;
-                    OD[w * kRound + rank] =
-                        (int)((uint32_t)lane | head << 8 | tail << 9 | (valid ? 0u : 1u) << 10 | bin << 16);
-                }
-            }
-            // the partial Grams are complete: every producer warp builds rows
-            // of the round's system. The round's errors solve err = C - M err
-            // with M unit lower triangular: M_ji (i < j) is the effect of
-            // err_i on rating j through q (a_i^(j-1-i) G_ij), the q^f row of a
-            // shared bin (a_f^(same-bin ratings between) G_ij) and the item
-            // biases. Warp pw takes rows i = pw, pw + 8, ... with j = lane.
-            asm volatile("bar.sync 2, %0;" ::"r"(kPW * 32) : "memory");
-            static_assert(kGW == 4, "the Gram partials are summed as (0 + 1) + (2 + 3)");
-#pragma unroll
-            for (int ps = 0; ps < kRound / kPW; ++ps) {
-                const int ii = ps * kPW + pw, jj = lane;
-                const uint32_t ki = __shfl_sync(kFull, mine.key, ii), kj = mine.key;
-                if (ii < jj) {
-                    float v = 0.0f;
-                    if (jj < (int)m) {
-                        const size_t ge = (size_t)ii * kGS + jj, gs = (size_t)kRound * kGS;
-                        const float g = (gp[ge] + gp[gs + ge]) + (gp[2 * gs + ge] + gp[3 * gs + ge]);
-                        const float cui = dst[(size_t)ii * stride + Fs + 1], cuj = dst[(size_t)jj * stride + Fs + 1];
-                        const bool same_f = rec_fbin(ki) == rec_fbin(kj), same_t = rec_tbin(ki) == rec_tbin(kj);
-                        const float bias_lr = p.lr_ib + (same_t ? p.lr_ti : 0.0f) + (same_f ? p.lr_ibf : 0.0f);
-                        const unsigned between = ((1u << jj) - 1u) & ~((2u << ii) - 1u);
-                        v = cuj * cui * bias_lr + p.lr_i * apow[jj - 1 - ii] * g +
-                            (same_f ? p.lr_iqf * fpow[__popc(same & between)] * g : 0.0f);
-                    }
-                    Mb[(size_t)jj * kMS + ii] = v;
-                    Mb[(size_t)ii * kMS + jj] = 0.0f;
-                } else if (ii == jj) {
-                    Mb[(size_t)ii * kMS + ii] = 0.0f;
-                }
+                // the previous rating of the same bin in the round, or -1
+                V[7 * kRound + lane] = __int_as_float(earlier ? 31 - __clz((int)earlier) : -1);
+                V[8 * kRound + lane] = __uint_as_float(rec_tbin(mine.key));
             }
             // the next rounds' loads
             rc1 = rc2;
@@ -1179,71 +1147,79 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                     }
                     const float wq = valid ? p.lr_i * V[2 * kRound + lane] * x : 0.0f;
                     const float wf = valid ? p.lr_iqf * V[3 * kRound + lane] * x : 0.0f;
-                    ap[lane] = make_float4(wq, wf, V[4 * kRound + lane], __uint_as_float(fbl));
+                    const int pv = __float_as_int(V[7 * kRound + lane]);
+                    ap[lane] = make_float4(wq, wf, V[4 * kRound + lane], __uint_as_float(fbl | (uint32_t)(pv + 1) << 8));
                     wb = valid ? x * cu_t : 0.0f;
                     sv[2 * kRound + lane] = wb;
                 }
                 asm volatile("bar.sync 1, %0;" ::"r"(kCW * 32) : "memory");
-                // q: q_m = a_i^m q_0 - sum_j w_j pe_j, in rating order (the
-                // weights of ratings past m are zero)
+                // q and q^f stripes, kChunk ratings at a time: the chunk's pe
+                // and q^f values are loaded together, a rating whose bin an
+                // earlier rating of the chunk updated takes that value from
+                // registers, and the chunk's rows are stored at its end.
                 const float am = V[6 * kRound];
 #pragma unroll
                 for (int t = 0; t < CPL; ++t) qv[t] *= am;
-#pragma unroll 4
-                for (int j = 0; j < kRound; ++j) {
-                    const float wq = ap[j].x;
+#pragma unroll 1
+                for (int c0 = 0; c0 < kRound; c0 += kChunk) {
+                    float pk[kChunk][CPL], ol[kChunk][CPL], nv[kChunk][CPL];
+                    float4 w4[kChunk];
 #pragma unroll
-                    for (int t = 0; t < CPL; ++t) {
-                        const uint32_t sc = warp + kCW * t;
-                        if (sc < NS) qv[t] = fmaf(-wq, src[(size_t)j * stride + 32 * sc + lane], qv[t]);
-                    }
-                }
-                // q^f rows: each bin's ratings in rating order (the order by
-                // bin is stable), the first applying the decay of all of them,
-                // qf_b = a_f^(n_b) qf_b - sum_j lr_iqf a_f^(later of bin) err_j pe_j;
-                // every bin row is read once and written once
-                const int* OD = od + (size_t)(r & 1) * 2 * kRound;
-                {
-                    float acc[CPL];
-#pragma unroll
-                    for (int t = 0; t < CPL; ++t) acc[t] = 0.0f;
-#pragma unroll 4
-                    for (int s2 = 0; s2 < kRound; ++s2) {
-                        const uint32_t o = (uint32_t)OD[s2];
-                        if (o & (1u << 10)) break;  // ratings past m come last
-                        const uint32_t j = o & 31u, fb = o >> 16;
-                        const float4 w4 = ap[j];
+                    for (int u = 0; u < kChunk; ++u) {
+                        w4[u] = ap[c0 + u];
+                        const uint32_t fk = __float_as_uint(w4[u].w) & 0xffu;
 #pragma unroll
                         for (int t = 0; t < CPL; ++t) {
                             const uint32_t sc = warp + kCW * t;
-                            if (sc < NS) {
-                                float* row = qfs + (size_t)fb * qs + 32 * sc + lane;
-                                if (o & (1u << 8)) acc[t] = w4.z * *row;
-                                acc[t] = fmaf(-w4.y, src[(size_t)j * stride + 32 * sc + lane], acc[t]);
-                                if (o & (1u << 9)) *row = acc[t];
-                            }
+                            pk[u][t] = sc < NS ? src[(size_t)(c0 + u) * stride + 32 * sc + lane] : 0.0f;
+                            ol[u][t] = sc < NS ? qfs[(size_t)fk * qs + 32 * sc + lane] : 0.0f;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kChunk; ++u) {
+                        const float wq = w4[u].x, wf = w4[u].y, dk = w4[u].z;
+                        const int pv = (int)(__float_as_uint(w4[u].w) >> 8) - 1;
+#pragma unroll
+                        for (int t = 0; t < CPL; ++t) {
+                            qv[t] = fmaf(-wq, pk[u][t], qv[t]);
+                            float o = ol[u][t];
+#pragma unroll
+                            for (int u2 = 0; u2 < u; ++u2) o = pv == c0 + u2 ? nv[u2][t] : o;
+                            nv[u][t] = fmaf(-wf, pk[u][t], dk * o);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kChunk; ++u) {
+                        // (ratings m..31 of a partial round would store stale rows)
+                        if (c0 + u >= (int)m) break;
+                        const uint32_t fk = __float_as_uint(w4[u].w) & 0xffu;
+#pragma unroll
+                        for (int t = 0; t < CPL; ++t) {
+                            const uint32_t sc = warp + kCW * t;
+                            if (sc < NS) qfs[(size_t)fk * qs + 32 * sc + lane] = nv[u][t];
                         }
                     }
                 }
                 if (warp < 2) {
                     // item biases: warp 0 the item bias and the time-bin
-                    // biases, warp 1 the frequency-bin biases, each bin's
-                    // err_j cu_j summed over its ratings in rating order
+                    // biases, warp 1 the frequency-bin biases
                     if (warp == 0) {
                         const float sw = warp_sum(wb);
                         if (lane == 0) sst[0] = sst[0] - p.lr_ib * sw;
                     }
-                    const int* O2 = OD + (warp == 0 ? kRound : 0);
-                    float* bb = sst + (warp == 0 ? 1 : 65);
-                    const float lr = warp == 0 ? p.lr_ti : p.lr_ibf;
-                    float bs = 0.0f;
-                    for (int s2 = 0; s2 < kRound; ++s2) {
-                        const uint32_t o = (uint32_t)O2[s2];
-                        if (o & (1u << 10)) break;
-                        const float e = sv[2 * kRound + (o & 31u)];
-                        bs = (o & (1u << 8)) ? 0.0f + e : bs + e;
-                        if ((o & (1u << 9)) && lane == 0) bb[o >> 16] = bb[o >> 16] - lr * bs;
+                    const int vo = warp == 0 ? 8 : 5;  // the ratings' bins: tb (vector 8) or fb (vector 5)
+                    float d0 = 0.0f, d1 = 0.0f;
+#pragma unroll 8
+                    for (int c = 0; c < kRound; ++c) {
+                        const float e = sv[2 * kRound + c];
+                        const uint32_t bk = __float_as_uint(V[vo * kRound + c]);
+                        d0 += lane == (int)bk ? e : 0.0f;
+                        d1 += lane + 32 == (int)bk ? e : 0.0f;
                     }
+                    const float lr = warp == 0 ? p.lr_ti : p.lr_ibf;
+                    float* bb = sst + (warp == 0 ? 1 : 65);
+                    bb[lane] = bb[lane] - lr * d0;
+                    bb[lane + 32] = bb[lane + 32] - lr * d1;
                 }
             }
             __syncthreads();

@@ -55,6 +55,11 @@ def calc_subscores(model, ds: Dataset) -> np.ndarray:
     return model.predict_subscores_batch(ds.user_idxs, ds.item_idxs, ds.dates)
 
 
+def fmt5(x: float) -> str:
+    """`{:.5}` of an f64 as Rust formats it (NaN is "NaN")."""
+    return "NaN" if x != x else f"{x:.5f}"
+
+
 def report_rmse(model, epoch: int, n_epochs: int, ds: Dataset, tee: Tee):
     """src/lib.rs:676-686"""
     tee.write(f"Epoch {epoch:02d}")
@@ -62,7 +67,7 @@ def report_rmse(model, epoch: int, n_epochs: int, ds: Dataset, tee: Tee):
         tee.write("\n")
         return None
     r = calc_rmse(model, ds)
-    tee.write(f" | RMSE {r:.5f}\n")
+    tee.write(f" | RMSE {fmt5(r)}\n")
     return r
 
 
@@ -149,7 +154,7 @@ def fit2_inner(model_factory, cfg, model_name: str, sets: dict, preds_dir: str, 
         model, curve = _train(model_factory, cfg, tr, pr, model_name, preds_dir, opts.save_probe_each_epoch, prn,
                               tee, qual, qual_name)
         pr_preds = gen_preds_parallel(model, pr)
-        tee.write(f"{prn} RMSE {rmse_from_preds(pr_preds, pr):.5f}\n")
+        tee.write(f"{prn} RMSE {fmt5(rmse_from_preds(pr_preds, pr))}\n")
         np.save(os.path.join(preds_dir, f"{model_name}.{prn}.npy"), pr_preds)
         if opts.save_subscores and model.n_subscores() > 0:
             _save_subscores(model, pr, model_name, prn, preds_dir)

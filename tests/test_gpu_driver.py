@@ -103,7 +103,9 @@ def test_fit2_inner_outputs_match_the_oracle_run(tmp_path, tiny, no_fulltrain):
     for a, b in zip(gl, ol):
         if "RMSE" in a:
             assert a.split("RMSE")[0] == b.split("RMSE")[0]
-            assert abs(float(a.split("RMSE")[1]) - float(b.split("RMSE")[1])) < 1e-4
+            x, y = float(a.split("RMSE")[1]), float(b.split("RMSE")[1])
+            # a set of test rows only (qual) has no RMSE: NaN, printed "NaN"
+            assert (x != x and y != y and a.endswith("NaN")) or abs(x - y) < 1e-4, (a, b)
         elif a.startswith("Saved item factors to "):
             assert os.path.basename(a) == os.path.basename(b)
         else:

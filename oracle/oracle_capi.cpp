@@ -173,6 +173,16 @@ int orc_fit_epoch(void* p, uint64_t epoch, int schedule, float nsvd_norm_exp, ui
     });
 }
 
+// Schedule 1 with one chunk (n_threads = 1), computed on `workers` host
+// threads; the same arithmetic in the same order (low_memory only).
+int orc_fit_epoch_p_workers(void* p, uint64_t epoch, float nsvd_norm_exp, uint64_t workers) {
+    Handle* h = (Handle*)p;
+    return guard([&] {
+        if (h->fp64) h->m64->fit_epoch_p_workers(h->tr.v, h->pr.v, epoch, nsvd_norm_exp, workers);
+        else h->m32->fit_epoch_p_workers(h->tr.v, h->pr.v, epoch, nsvd_norm_exp, workers);
+    });
+}
+
 // The parallel schedule in the steps a sharded run takes (src/tsvdx4p.rs:
 // fit_epoch_user :390-639 restricted to the users u_lo..u_hi-1, in the epoch's
 // order; apply_nsvd_deltas :341-385 of deltas summed elsewhere; fit_epoch_item

@@ -36,6 +36,7 @@ def lib():
         L.orc_create.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.orc_destroy.argtypes = [C.c_void_p]
         L.orc_fit_epoch.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_float, C.c_uint64]
+        L.orc_fit_epoch_p_workers.argtypes = [C.c_void_p, C.c_uint64, C.c_float, C.c_uint64]
         L.orc_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]
         L.orc_predict_subscores.argtypes = L.orc_predict.argtypes
         L.orc_calc_rmse.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
@@ -91,6 +92,11 @@ class OracleModel:
 
     def fit_epoch(self, epoch: int, schedule: int = SCHED_SEQ, nsvd_norm_exp: float = 1.0, n_threads: int = 1):
         _check(lib().orc_fit_epoch(self.h, epoch, schedule, nsvd_norm_exp, n_threads))
+
+    def fit_epoch_parallel(self, epoch: int, nsvd_norm_exp: float = 1.0, workers: int = 4):
+        """SCHED_P with one chunk, on `workers` host threads (same arithmetic,
+        same order; low_memory configurations only)."""
+        _check(lib().orc_fit_epoch_p_workers(self.h, epoch, nsvd_norm_exp, workers))
 
     def predict_batch(self, u, i, day):
         u = np.ascontiguousarray(u, np.int32)

@@ -21,6 +21,7 @@
 // FP64 twin used to state the error of reduced-precision forms.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include <math.h>
 
 #include <cmath>
@@ -28,6 +29,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rand09.hpp"
@@ -697,7 +699,11 @@ struct TxModel {
 
     // The user phase for `users` in the given order, accumulating their NSVD1
     // deltas into d (src/tsvdx4p.rs:449-630, one chunk's loop).
-    void user_phase_p(const DataView& tr, const DataView& pr, const std::vector<uint32_t>& users, PDeltas& d) {
+    // With sv and se given (low_memory only), each user's delta row seq / norm
+    // and sum_err / norm are written to sv[u * F ..] and se[u] instead of
+    // being added into d, for a caller that sums them per item in user order.
+    void user_phase_p(const DataView& tr, const DataView& pr, const std::vector<uint32_t>& users, PDeltas& d,
+                      T* sv = nullptr, T* se = nullptr) {
         const Config c = cfg;
         const size_t F = c.n_feat, NF = c.n_freq_bins;
         const bool low_mem = c.low_memory, use_probe = c.full_su;
@@ -814,6 +820,11 @@ struct TxModel {
                         ++dr_idx;
                     }
                 }
+                if (sv) {
+                    for (size_t k = 0; k < F; ++k) sv[u * F + k] = seq[k] / norm;
+                    se[u] = sum_err / norm;
+                    continue;
+                }
                 for (size_t t = start; t < end; ++t) {
                     size_t j = tr.item_idxs[t];
                     for (size_t k = 0; k < F; ++k) dy.at(j, k) += seq[k] / norm;
@@ -822,6 +833,110 @@ struct TxModel {
                 }
             }
         }
+    }
+
+    // fit_epoch_user_p with one chunk followed by fit_epoch_item_p, on
+    // `workers` host threads, with the same arithmetic in the same order:
+    // users' SGD in parallel slices of the epoch's order (item tables are
+    // frozen in the user phase), each item's delta sum over the users in the
+    // epoch's order (items split between the threads), the y update, the
+    // cache rebuild per user (its train then probe rows in order) and the
+    // item phase per item. low_memory only.
+    void fit_epoch_p_workers(const DataView& tr, const DataView& pr, uint64_t epoch, float nsvd_norm_exp,
+                             size_t workers) {
+        const Config c = cfg;
+        if (!c.low_memory) throw std::runtime_error("fit_epoch_p_workers: low_memory only");
+        const size_t F = c.n_feat;
+        workers = std::max<size_t>(workers, 1);
+        auto par = [&](size_t n, auto&& body) {  // body(w, lo, hi) over n units in `workers` slices
+            std::vector<std::thread> th;
+            const size_t per = (n + workers - 1) / workers;
+            for (size_t w = 0; w < workers; ++w) {
+                const size_t lo = std::min(n, w * per), hi = std::min(n, lo + per);
+                th.emplace_back([&, w, lo, hi] { body(w, lo, hi); });
+            }
+            for (auto& t : th) t.join();
+        };
+        user_phase_prologue_p(epoch);
+        const std::vector<uint32_t> users = users_for_epoch(epoch);
+        std::vector<T> sv(n_users * F, T(0)), se(n_users, T(0));
+        par(users.size(), [&](size_t, size_t lo, size_t hi) {
+            PDeltas scratch(0, F, false);
+            std::vector<uint32_t> part(users.begin() + lo, users.begin() + hi);
+            user_phase_p(tr, pr, part, scratch, sv.data(), se.data());
+        });
+        PDeltas tot(n_items, F, false);
+        const std::vector<size_t> offs = calc_user_offsets(tr);
+        par(n_items, [&](size_t, size_t j_lo, size_t j_hi) {
+            for (uint32_t u : users)
+                for (size_t t = offs[u]; t < offs[u + 1]; ++t) {
+                    const size_t j = tr.item_idxs[t];
+                    if (j < j_lo || j >= j_hi) continue;
+                    for (size_t k = 0; k < F; ++k) tot.dy.at(j, k) += sv[u * F + k];
+                    tot.dyb[j] += se[u];
+                    tot.nc[j] += 1;
+                }
+        });
+        apply_deltas_p_workers(tr, pr, tot, nsvd_norm_exp, par);
+        if (by_item.starts.empty()) build_by_item(tr);
+        std::vector<size_t> order(n_items);
+        for (size_t i = 0; i < n_items; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+            return by_item.starts[x + 1] - by_item.starts[x] > by_item.starts[y + 1] - by_item.starts[y];
+        });
+        std::atomic<size_t> next{0};
+        par(workers, [&](size_t, size_t, size_t) {
+            for (size_t k; (k = next.fetch_add(1)) < n_items;) item_phase_p(tr, order[k], order[k] + 1);
+        });
+    }
+
+    // apply_deltas_p with the cache rebuild split over users.
+    template <class Par>
+    void apply_deltas_p_workers(const DataView& tr, const DataView& pr, const PDeltas& tot, float nsvd_norm_exp,
+                                Par&& par) {
+        const Config c = cfg;
+        const size_t F = c.n_feat;
+        const float ex = nsvd_norm_exp;
+        for (size_t j = 0; j < n_items; ++j) {
+            if (tot.nc[j] == 0) continue;
+            T scale = ex == 0.0f ? T(1) : powT((T)(float)tot.nc[j], (T)ex);
+            for (size_t k = 0; k < F; ++k) {
+                T yj = yfeat.at(j, k);
+                yfeat.at(j, k) -= (T)c.lr_y * (tot.dy.at(j, k) / scale + (T)c.reg_y * yj);
+            }
+            ybias[j] -= (T)c.lr_yb * (tot.dyb[j] / scale);
+        }
+        // each user's train rows, then its probe rows, in row order (the
+        // probe set need not be user-sorted)
+        std::vector<size_t> off(n_users + 1, 0);
+        for (size_t t = 0; t < tr.n_ratings; ++t) ++off[tr.user_idxs[t] + 1];
+        for (size_t t = 0; t < pr.n_ratings; ++t) ++off[pr.user_idxs[t] + 1];
+        for (size_t u = 0; u < n_users; ++u) off[u + 1] += off[u];
+        std::vector<uint32_t> items(off[n_users]);
+        {
+            std::vector<size_t> at(off.begin(), off.end() - 1);
+            for (size_t t = 0; t < tr.n_ratings; ++t) items[at[tr.user_idxs[t]]++] = (uint32_t)tr.item_idxs[t];
+            for (size_t t = 0; t < pr.n_ratings; ++t) items[at[pr.user_idxs[t]]++] = (uint32_t)pr.item_idxs[t];
+        }
+        par(n_users, [&](size_t, size_t u_lo, size_t u_hi) {
+            for (size_t u = u_lo; u < u_hi; ++u) {
+                T* su = ycache.row(u);
+                T sb = T(0);
+                for (size_t k = 0; k < F; ++k) su[k] = T(0);
+                for (size_t e = off[u]; e < off[u + 1]; ++e) {
+                    const T* y = yfeat.row(items[e]);
+                    for (size_t k = 0; k < F; ++k) su[k] += y[k];
+                    sb += ybias[items[e]];
+                }
+                const int32_t cnt = tr.user_cnts[u] + pr.user_cnts[u];
+                if (cnt > 0) {
+                    const T nrm = sqrtT((T)(float)cnt);
+                    for (size_t k = 0; k < F; ++k) su[k] /= nrm;
+                    sb /= nrm;
+                }
+                ycache_bias[u] = sb;
+            }
+        });
     }
 
     // apply_nsvd_deltas (src/tsvdx4p.rs:341-385) of the summed deltas, then

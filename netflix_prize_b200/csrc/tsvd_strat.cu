@@ -1157,6 +1157,29 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                 // and q^f values are loaded together, a rating whose bin an
                 // earlier rating of the chunk updated takes that value from
                 // registers, and the chunk's rows are stored at its end.
+                if (warp >= 2) {
+                    // item biases, beside the q and q^f updates of warps 0
+                    // and 1 (at f <= 64 warps 2 and 3 hold no stripes): warp 2
+                    // the item bias and the time-bin biases, warp 3 the
+                    // frequency-bin biases
+                    if (warp == 2) {
+                        const float sw = warp_sum(sv[2 * kRound + lane]);
+                        if (lane == 0) sst[0] = sst[0] - p.lr_ib * sw;
+                    }
+                    const int vo = warp == 2 ? 8 : 5;  // the ratings' bins: tb (vector 8) or fb (vector 5)
+                    float d0 = 0.0f, d1 = 0.0f;
+#pragma unroll 8
+                    for (int c = 0; c < kRound; ++c) {
+                        const float e = sv[2 * kRound + c];
+                        const uint32_t bk = __float_as_uint(V[vo * kRound + c]);
+                        d0 += lane == (int)bk ? e : 0.0f;
+                        d1 += lane + 32 == (int)bk ? e : 0.0f;
+                    }
+                    const float lr = warp == 2 ? p.lr_ti : p.lr_ibf;
+                    float* bb = sst + (warp == 2 ? 1 : 65);
+                    bb[lane] = bb[lane] - lr * d0;
+                    bb[lane + 32] = bb[lane + 32] - lr * d1;
+                }
                 const float am = V[6 * kRound];
 #pragma unroll
                 for (int t = 0; t < CPL; ++t) qv[t] *= am;
@@ -1199,27 +1222,6 @@ __global__ void __launch_bounds__(kItemThreads, 1) k_item_pass(DeviceState s, Ep
                             if (sc < NS) qfs[(size_t)fk * qs + 32 * sc + lane] = nv[u][t];
                         }
                     }
-                }
-                if (warp < 2) {
-                    // item biases: warp 0 the item bias and the time-bin
-                    // biases, warp 1 the frequency-bin biases
-                    if (warp == 0) {
-                        const float sw = warp_sum(wb);
-                        if (lane == 0) sst[0] = sst[0] - p.lr_ib * sw;
-                    }
-                    const int vo = warp == 0 ? 8 : 5;  // the ratings' bins: tb (vector 8) or fb (vector 5)
-                    float d0 = 0.0f, d1 = 0.0f;
-#pragma unroll 8
-                    for (int c = 0; c < kRound; ++c) {
-                        const float e = sv[2 * kRound + c];
-                        const uint32_t bk = __float_as_uint(V[vo * kRound + c]);
-                        d0 += lane == (int)bk ? e : 0.0f;
-                        d1 += lane + 32 == (int)bk ? e : 0.0f;
-                    }
-                    const float lr = warp == 0 ? p.lr_ti : p.lr_ibf;
-                    float* bb = sst + (warp == 0 ? 1 : 65);
-                    bb[lane] = bb[lane] - lr * d0;
-                    bb[lane + 32] = bb[lane + 32] - lr * d1;
                 }
             }
             __syncthreads();

@@ -19,6 +19,11 @@ single-threaded). The output file is rewritten after every epoch, so a run
 that stops early leaves the epochs it finished.
 
   python tests/golden/make_rmse_curves.py --case c1_f32
+  python tests/golden/make_rmse_curves.py --case c2_f64 --schedule p --workers 6
+
+The second form writes the curve of the reference's parallel model
+(rmse_curve_<case>_p.json), the algorithm the GPU's stratified schedule
+restates, on host threads (bitwise the one-thread result).
 """
 from __future__ import annotations
 
@@ -65,7 +70,8 @@ def main():
     ap.add_argument("--case", choices=sorted(CASES), required=True)
     ap.add_argument("--out", default=None)
     ap.add_argument("--schedule", choices=["seq", "p"], default="seq",
-                    help="seq: TxModel::fit_epoch; p: Tsvdx4pModel (src/tsvdx4p.rs:815-822)")
+                    help="seq: TxModel::fit_epoch; p: Tsvdx4pModel (src/tsvdx4p.rs:815-822), one chunk")
+    ap.add_argument("--workers", type=int, default=1, help="host threads of the p schedule (same result)")
     args = ap.parse_args()
     from netflix_prize_b200.data import MaskedDataset
     from oracle import pyoracle as po
@@ -80,7 +86,8 @@ def main():
         "case": args.case,
         "algorithm": ("TxModel::fit_epoch (src/tx.rs:734-1115), sequential, C++ restatement, 1 thread"
                       if args.schedule == "seq" else
-                      "Tsvdx4pModel::fit_epoch (src/tsvdx4p.rs:815-822), C++ restatement, 1 thread"),
+                      "Tsvdx4pModel::fit_epoch (src/tsvdx4p.rs:815-822), one chunk, NSVD1 norm exponent 1, "
+                      "C++ restatement"),
         "generator": {"spec": spec.__dict__.copy(), "fingerprint": fingerprint(tr, pr),
                       "n_train": int(tr.n_ratings), "n_pr": int(pr.n_ratings),
                       "n_heldout": int((pr.is_test == 0).sum())},
@@ -92,7 +99,10 @@ def main():
     sched = po.SCHED_SEQ if args.schedule == "seq" else po.SCHED_P
     for e in range(1, cfg.n_epochs + 1):
         t = time.time()
-        m.fit_epoch(e, sched, nsvd_norm_exp=1.0, n_threads=1)
+        if sched == po.SCHED_SEQ:
+            m.fit_epoch(e, sched)
+        else:
+            m.fit_epoch_parallel(e, nsvd_norm_exp=1.0, workers=args.workers)
         fit_s = time.time() - t
         r = m.calc_rmse(pr)
         rec["epochs"].append({"epoch": e, "heldout_rmse": r, "fit_s": round(fit_s, 2)})

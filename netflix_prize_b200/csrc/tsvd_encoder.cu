@@ -15,10 +15,11 @@
 //
 // Loss: mean squared error against the standardised targets. Weights are FP32
 // masters with BF16 copies; every GEMM runs on the tensor cores with BF16
-// operands and an FP32 accumulator in tensor memory (tcgen05.mma, 128x128
-// tiles), activations are stored as BF16 for the next GEMM and as FP32
+// operands and an FP32 accumulator in tensor memory (tcgen05.mma, 128x64
+// tiles, operands brought by TMA), activations are stored as BF16 for the next GEMM and as FP32
 // pre-activations for the GELU derivative. AdamW updates all parameters
 // (weight decay on the matrices).
+#include <cuda.h>  // CUtensorMap and the tensor-map encoder (reached through the runtime's driver entry point)
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -62,8 +63,9 @@ __device__ __forceinline__ float gelu_grad(float x) {
 }
 
 // ---------------------------------------------------------------------------
-// The GEMM runs on the 5th-generation tensor cores (tcgen05): a 128x64 output
-// tile per CTA with its FP32 accumulator in tensor memory. Each 64-deep K block
+// The register-staged GEMM (k_gemm_tc; k_gemm_tma below is the TMA-fed form
+// that gemm() prefers) runs on the 5th-generation tensor cores (tcgen05): a
+// 128x64 output tile per CTA with its FP32 accumulator in tensor memory. Each 64-deep K block
 // of A and B is staged in shared memory as BF16 in the K-major, unswizzled
 // core-matrix layout (a core matrix is 8 rows x 16 bytes; core matrices are
 // 128 B apart along K and 1024 B apart along M or N). Two stages: while one
@@ -377,12 +379,203 @@ __global__ void k_splitk_sum(const float* __restrict__ ws, int splits, int M, in
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed GEMM (k_gemm_tma) for K-major operands with 16-byte aligned rows
+// (gemm() transposes MN-major operands into a workspace first). Each K block
+// of A (128 rows) and B (64 rows) arrives as eight cp.async.bulk.tensor 2-D
+// tile loads of 8 K-columns x all rows of the tile (16 bytes per row): box g
+// lands at g x ROWS x 16 bytes, which is the K-major no-swizzle core-matrix
+// layout with K-adjacent core matrices ROWS x 16 bytes apart (LBO) and M- or
+// N-adjacent ones 128 bytes apart (SBO). The tensor maps' bounds give the zero
+// fill past M, N and K. kTmaStages stages: thread 0 issues a stage's loads
+// once the MMAs of its previous use have committed (the stage's empty
+// barrier); thread 32 issues the stage's four MMAs (M = 128, N = 64, K = 16)
+// once its loads have landed (full barrier, transaction bytes) and commits
+// them to the empty barrier; the last commit releases the epilogue. Every wait
+// is bounded; a wait that gives up sets *err and the kernel carries on, so all
+// issued work drains before the block exits. No multicast.
+// ---------------------------------------------------------------------------
+constexpr int kTmaStages = 4;
+constexpr uint32_t kTmaSmem = kTmaStages * kTcStage + 128;  // stages, 2 x kTmaStages + 1 mbarriers, TMEM address
+constexpr uint32_t kTmaLboA = TC_M * 16, kTmaLboB = TC_N * 16, kTmaSbo = 128;
+
+__device__ __forceinline__ uint64_t tma_desc(uint32_t addr, uint32_t lbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((kTmaSbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ void tma_tile(uint32_t dst, const CUtensorMap* map, int c0, int c1, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(mbar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tma(const __grid_constant__ CUtensorMap tmA,
+                                                  const __grid_constant__ CUtensorMap tmB, GemmArgs g,
+                                                  unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) uint8_t tsm[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(tsm + kTmaStages * kTcStage);
+    uint64_t* empty = full + kTmaStages;
+    uint64_t* done = empty + kTmaStages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * TC_N;
+    const uint32_t s_base = smem_u32(tsm);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)TC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int b = 0; b < 2 * kTmaStages + 1; ++b)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + b)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // split K as in k_gemm_tc: block z takes K blocks kb0 .. kb0 + nk - 1
+    const int nk_all = (g.K + TC_K - 1) / TC_K;
+    const int per = (nk_all + (int)gridDim.z - 1) / (int)gridDim.z;
+    const int kb0 = (int)blockIdx.z * per;
+    const int nk = min(nk_all, kb0 + per) - kb0;
+    float* const out_f32 = g.out_f32 ? g.out_f32 + (size_t)blockIdx.z * g.M * g.ldc : nullptr;
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+    if (tid == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+        for (int kb = 0; kb < nk; ++kb) {
+            const int st = kb % kTmaStages, use = kb / kTmaStages;
+            if (use > 0 && !tc_wait(smem_u32(empty + st), (uint32_t)((use - 1) & 1))) atomicOr(err, 1u);
+            const uint32_t fb = smem_u32(full + st);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(kTcStage) : "memory");
+            const uint32_t a_s = s_base + (uint32_t)st * kTcStage, b_s = a_s + kTcABytes;
+            const int k0 = (kb0 + kb) * TC_K;
+#pragma unroll
+            for (int g8 = 0; g8 < TC_K / 8; ++g8) {
+                tma_tile(a_s + (uint32_t)g8 * kTmaLboA, &tmA, k0 + 8 * g8, m0, fb);
+                tma_tile(b_s + (uint32_t)g8 * kTmaLboB, &tmB, k0 + 8 * g8, n0, fb);
+            }
+        }
+    } else if (tid == 32) {
+        for (int kb = 0; kb < nk; ++kb) {
+            const int st = kb % kTmaStages, use = kb / kTmaStages;
+            if (!tc_wait(smem_u32(full + st), (uint32_t)(use & 1))) atomicOr(err, 1u);
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a_s = s_base + (uint32_t)st * kTcStage, b_s = a_s + kTcABytes;
+#pragma unroll
+            for (int kk = 0; kk < TC_K / 16; ++kk) {
+                const uint64_t ad = tma_desc(a_s + (uint32_t)kk * 2u * kTmaLboA, kTmaLboA);
+                const uint64_t bd = tma_desc(b_s + (uint32_t)kk * 2u * kTmaLboB, kTmaLboB);
+                const uint32_t accumulate = (kb > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{.reg .pred p; setp.ne.u32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;}" ::"r"(
+                        tmem),
+                    "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(accumulate));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(empty + st))
+                         : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(done))
+                     : "memory");
+    }
+    __syncwarp();
+    const bool ok = __syncthreads_and(tc_wait(smem_u32(done), 0u) ? 1 : 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok) {
+        if (tid == 0) atomicOr(err, 1u);
+    } else {
+        const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_N; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < g.M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= g.N) continue;
+                    float x = __uint_as_float(v[j]);
+                    if (g.bias) x += g.bias[n];
+                    if (out_f32) out_f32[(size_t)m * g.ldc + n] = x;
+                    if (g.out_bf16) g.out_bf16[(size_t)m * g.ldc + n] = __float2bfloat16(g.gelu ? gelu_f(x) : x);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TC_N));
+}
+
+// out[c][r] = in[r][c] (r < R, c < C); in has leading dimension ld_in, out ld_out.
+__global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ in, int R, int C, int ld_in,
+                                 __nv_bfloat16* __restrict__ out, int ld_out) {
+    __shared__ __nv_bfloat16 t[32][34];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int r = r0 + y, c = c0 + threadIdx.x;
+        if (r < R && c < C) t[y][threadIdx.x] = in[(size_t)r * ld_in + c];
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int c = c0 + y, r = r0 + threadIdx.x;
+        if (c < C && r < R) out[(size_t)c * ld_out + r] = t[threadIdx.x][y];
+    }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// Tensor map of a K-major BF16 operand X[rows][K] (leading dimension ld, a
+// multiple of 8; 16-byte aligned base): boxes of 8 K-columns x box_rows rows.
+bool k_major_map(CUtensorMap* map, const __nv_bfloat16* X, int K, int rows, int ld, int box_rows) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+    const cuuint32_t es[2] = {1u, 1u};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(X), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // `err` receives 1 when an MMA completion wait ran out (the results are then invalid).
 // splits > 1 (FP32 output only, no bias or activation) divides K over that many
 // blocks per tile, through ws (splits * M * ldc floats), summed in a fixed order.
+// tws (tws_elems BF16 elements) takes the transposed copies of MN-major
+// operands for the TMA path; without room there, or with operands whose rows
+// are not 16-byte aligned, the register-staged kernel runs instead.
 void gemm(cudaStream_t st, unsigned* err, const __nv_bfloat16* A, int a_km, int lda, const __nv_bfloat16* B, int b_kn, int ldb, int M,
           int N, int K, const float* bias, float* out_f32, __nv_bfloat16* out_bf16, int ldc, int gelu, int splits = 1,
-          float* ws = nullptr) {
+          float* ws = nullptr, __nv_bfloat16* tws = nullptr, size_t tws_elems = 0) {
     // K = 0 would issue no MMA and leave the accumulator uninitialised
     if (M <= 0 || N <= 0 || K <= 0) throw Error(TSVD_ERR_INVALID, "gemm: M, N and K must be positive");
     const int nk = (K + TC_K - 1) / TC_K;
@@ -393,11 +586,48 @@ void gemm(cudaStream_t st, unsigned* err, const __nv_bfloat16* A, int a_km, int 
     }
     const bool split = splits > 1 && ws && out_f32 && !bias && !out_bf16 && !gelu;
     if (!split) splits = 1;
-    GemmArgs g{A, B, M, N, K, lda, ldb, a_km, b_kn, bias, split ? ws : out_f32, out_bf16, ldc, gelu};
-    TSVD_CUDA(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M, splits);
-    k_gemm_tc<<<grid, 128, kTcSmem, st>>>(g, err);
-    TSVD_CUDA(cudaGetLastError());
+    // TMA path: every operand K-major with 16-byte aligned rows, MN-major ones
+    // transposed into tws first (leading dimension K rounded up to 8)
+    const int k8 = (K + 7) & ~7;
+    const size_t need = (a_km ? (size_t)M * k8 : 0) + (b_kn ? (size_t)N * k8 : 0);
+    bool tma = encode_tiled() != nullptr && need <= (tws ? tws_elems : 0);
+    if (!a_km && ((lda & 7) || (reinterpret_cast<uintptr_t>(A) & 15))) tma = false;
+    if (!b_kn && ((ldb & 7) || (reinterpret_cast<uintptr_t>(B) & 15))) tma = false;
+    if (tma) {
+        const __nv_bfloat16* Ak = A;
+        const __nv_bfloat16* Bk = B;
+        int ldak = lda, ldbk = ldb;
+        __nv_bfloat16* p = tws;
+        const dim3 tb(32, 8);
+        if (a_km) {  // A stored [K][M]
+            k_transpose_bf16<<<dim3((M + 31) / 32, (K + 31) / 32), tb, 0, st>>>(A, K, M, lda, p, k8);
+            TSVD_CUDA(cudaGetLastError());
+            Ak = p;
+            ldak = k8;
+            p += (size_t)M * k8;
+        }
+        if (b_kn) {  // B stored [K][N]
+            k_transpose_bf16<<<dim3((N + 31) / 32, (K + 31) / 32), tb, 0, st>>>(B, K, N, ldb, p, k8);
+            TSVD_CUDA(cudaGetLastError());
+            Bk = p;
+            ldbk = k8;
+        }
+        CUtensorMap ma, mb;
+        tma = k_major_map(&ma, Ak, K, M, ldak, TC_M) && k_major_map(&mb, Bk, K, N, ldbk, TC_N);
+        if (tma) {
+            GemmArgs g{Ak, Bk, M, N, K, ldak, ldbk, 0, 0, bias, split ? ws : out_f32, out_bf16, ldc, gelu};
+            TSVD_CUDA(cudaFuncSetAttribute(k_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmem));
+            k_gemm_tma<<<grid, 128, kTmaSmem, st>>>(ma, mb, g, err);
+            TSVD_CUDA(cudaGetLastError());
+        }
+    }
+    if (!tma) {
+        GemmArgs g{A, B, M, N, K, lda, ldb, a_km, b_kn, bias, split ? ws : out_f32, out_bf16, ldc, gelu};
+        TSVD_CUDA(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        k_gemm_tc<<<grid, 128, kTcSmem, st>>>(g, err);
+        TSVD_CUDA(cudaGetLastError());
+    }
     if (split) {
         k_splitk_sum<<<(unsigned)std::min<size_t>(((size_t)M * N + 255) / 256, 148 * 8), 256, 0, st>>>(ws, splits, M, N, ldc,
                                                                                                     out_f32);
@@ -670,6 +900,8 @@ struct tsvd_encoder {
     tsvd::DevMem hist, inv_n;  // per batch user: rating and date-bin counts, 1 / history length
     tsvd::DevMem tc_err;       // set by the tensor-core GEMM when an MMA wait ran out
     tsvd::DevMem ws;           // split-K partial tiles of the weight-gradient GEMMs
+    tsvd::DevMem tws;          // transposed copies of MN-major GEMM operands (TMA path)
+    size_t tws_elems = 0;
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::string err;
@@ -713,11 +945,11 @@ void forward(tsvd_encoder* e, int n) {
                                               e->inv_n.as<float>());
     TSVD_CUDA(cudaGetLastError());
     gemm(st, e->tc_err.as<unsigned>(), e->h0b.as<__nv_bfloat16>(), 0, kEmb, P(e, 3).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kEmb,
-         P(e, 4).w.as<float>(), e->z1.as<float>(), e->h1b.as<__nv_bfloat16>(), kHid, 1);
+         P(e, 4).w.as<float>(), e->z1.as<float>(), e->h1b.as<__nv_bfloat16>(), kHid, 1, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 1, kHid, n, kHid, kHid,
-         P(e, 6).w.as<float>(), e->z2.as<float>(), e->h2b.as<__nv_bfloat16>(), kHid, 1);
+         P(e, 6).w.as<float>(), e->z2.as<float>(), e->h2b.as<__nv_bfloat16>(), kHid, 1, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 0, kHid, P(e, 7).wb.as<__nv_bfloat16>(), 1, e->Op, n, e->O, kHid,
-         P(e, 8).w.as<float>(), e->y.as<float>(), nullptr, e->O, 0);
+         P(e, 8).w.as<float>(), e->y.as<float>(), nullptr, e->O, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
 }
 
 // loss and gradients for n users in e->users (targets from the model)
@@ -735,26 +967,26 @@ double backward(tsvd_encoder* e, int n) {
     TSVD_CUDA(cudaGetLastError());
     // layer 3
     gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, Op, kHid, O, n, nullptr,
-         P(e, 7).g.as<float>(), nullptr, O, 0, 8, e->ws.as<float>());
+         P(e, 7).g.as<float>(), nullptr, O, 0, 8, e->ws.as<float>(), e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_colsum_f<<<(O + 127) / 128, 128, 0, st>>>(e->dy.as<float>(), n, O, P(e, 8).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dyb.as<__nv_bfloat16>(), 0, Op, P(e, 7).wb.as<__nv_bfloat16>(), 0, Op, n, kHid, O, nullptr,
-         e->dh2.as<float>(), nullptr, kHid, 0);
+         e->dh2.as<float>(), nullptr, kHid, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh2.as<float>(), e->z2.as<float>(), n * kHid,
                                                            e->dz2b.as<__nv_bfloat16>());
     // layer 2
     gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 1, kHid, e->dz2b.as<__nv_bfloat16>(), 1, kHid, kHid, kHid, n, nullptr,
-         P(e, 5).g.as<float>(), nullptr, kHid, 0, 4, e->ws.as<float>());
+         P(e, 5).g.as<float>(), nullptr, kHid, 0, 4, e->ws.as<float>(), e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz2b.as<__nv_bfloat16>(), n, kHid, P(e, 6).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dz2b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 0, kHid, n, kHid, kHid, nullptr,
-         e->dh1.as<float>(), nullptr, kHid, 0);
+         e->dh1.as<float>(), nullptr, kHid, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh1.as<float>(), e->z1.as<float>(), n * kHid,
                                                            e->dz1b.as<__nv_bfloat16>());
     // layer 1
     gemm(st, e->tc_err.as<unsigned>(), e->h0b.as<__nv_bfloat16>(), 1, kEmb, e->dz1b.as<__nv_bfloat16>(), 1, kHid, kEmb, kHid, n, nullptr,
-         P(e, 3).g.as<float>(), nullptr, kHid, 0, 16, e->ws.as<float>());
+         P(e, 3).g.as<float>(), nullptr, kHid, 0, 16, e->ws.as<float>(), e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz1b.as<__nv_bfloat16>(), n, kHid, P(e, 4).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dz1b.as<__nv_bfloat16>(), 0, kHid, P(e, 3).wb.as<__nv_bfloat16>(), 0, kHid, n, kEmb, kHid, nullptr,
-         e->dh0.as<float>(), nullptr, kEmb, 0);
+         e->dh0.as<float>(), nullptr, kEmb, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     // embeddings
     for (int k = 0; k < 3; ++k) TSVD_CUDA(cudaMemsetAsync(P(e, k).g.p, 0, P(e, k).n * 4, st));
     k_embag_bwd<<<n, kBagWarps * 32, 0, st>>>(s, e->raw.as<int8_t>(), e->users.as<uint32_t>(), n,
@@ -921,6 +1153,9 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->tc_err.alloc(4);
         // split-K slices: dW1 16 x 128 x 512, dW2 4 x 512 x 512, dW3 8 x 512 x O
         e->ws.alloc(std::max(std::max((size_t)16 * kEmb * kHid, (size_t)4 * kHid * kHid), (size_t)8 * kHid * O) * 4);
+        // two transposed operands of at most 512 rows x max(batch, 512) columns
+        e->tws_elems = (size_t)2 * kHid * std::max(kMaxBatch, kHid);
+        e->tws.alloc(e->tws_elems * 2);
         TSVD_CUDA(cudaMemset(e->tc_err.p, 0, 4));
         TSVD_CUDA(cudaDeviceSynchronize());
     });

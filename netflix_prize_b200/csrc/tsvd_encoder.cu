@@ -816,20 +816,65 @@ __global__ void k_gelu_bwd(const float* __restrict__ dh, const float* __restrict
 }
 
 // column sums of a [rows, cols] matrix (bias gradients)
-__global__ void k_colsum_f(const float* __restrict__ x, int rows, int cols, float* __restrict__ out) {
+// Column sums out[c] = sum_r x[r][c] (x [rows][cols]) in two fixed-order
+// levels, so that many blocks share the rows and the result does not depend on
+// scheduling: block (bx, by) sums rows by * kColRows .. of columns 32 bx ..
+// with 8 row lanes (rows r, r + 8, ... each) and adds the lanes in order into
+// part[by][c]; k_colsum_fin adds the row chunks in order.
+constexpr int kColRows = 256;
+
+template <class T>
+__device__ __forceinline__ float as_float(T v);
+template <>
+__device__ __forceinline__ float as_float<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float as_float<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <class T>
+__global__ void k_colsum_part(const T* __restrict__ x, int rows, int cols, float* __restrict__ part) {
+    __shared__ float sh[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = blockIdx.y * kColRows, r1 = min(rows, r0 + kColRows);
+    float a = 0.0f;
+    if (c < cols)
+        for (int r = r0 + (int)threadIdx.y; r < r1; r += 8) a += as_float<T>(x[(size_t)r * cols + c]);
+    sh[threadIdx.y][threadIdx.x] = a;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = 0.0f;
+#pragma unroll
+        for (int y = 0; y < 8; ++y) t += sh[y][threadIdx.x];
+        part[(size_t)blockIdx.y * cols + c] = t;
+    }
+}
+
+__global__ void k_colsum_fin(const float* __restrict__ part, int chunks, int cols, float* __restrict__ out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
     float a = 0.0f;
-    for (int r = 0; r < rows; ++r) a += x[(size_t)r * cols + c];
+    for (int k = 0; k < chunks; ++k) a += part[(size_t)k * cols + c];
     out[c] = a;
 }
 
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ x, int rows, int cols, float* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
-    float a = 0.0f;
-    for (int r = 0; r < rows; ++r) a += __bfloat162float(x[(size_t)r * cols + c]);
-    out[c] = a;
+// out = column sums of x [rows][cols] through the workspace part
+// (ceil(rows / kColRows) * cols floats)
+template <class T>
+void colsum(cudaStream_t st, const T* x, int rows, int cols, float* part, float* out) {
+    const int chunks = (rows + kColRows - 1) / kColRows;
+    k_colsum_part<T><<<dim3((cols + 31) / 32, chunks), dim3(32, 8), 0, st>>>(x, rows, cols, part);
+    k_colsum_fin<<<(cols + 127) / 128, 128, 0, st>>>(part, chunks, cols, out);
+    TSVD_CUDA(cudaGetLastError());
+}
+
+// The batch's mean squared error sse / count from the k_mse block partials
+// (added in block order), into loss[0]; with `acc`, also added to the epoch's
+// running sum loss[1].
+__global__ void k_loss(const double* __restrict__ part, int nb, double count, double* __restrict__ loss, int acc) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double sse = 0.0;
+    for (int b = 0; b < nb; ++b) sse += part[b];
+    loss[0] = sse / count;
+    if (acc) loss[1] += loss[0];
 }
 
 __global__ void k_adamw(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
@@ -898,6 +943,8 @@ struct tsvd_encoder {
     tsvd::DevMem raw, mean, inv_std, std_;
     tsvd::DevMem users, h0, h0b, z1, h1b, z2, h2b, y, t, dy, dyb, dh2, dz2b, dh1, dz1b, dh0, part;
     tsvd::DevMem hist, inv_n;  // per batch user: rating and date-bin counts, 1 / history length
+    tsvd::DevMem loss;         // {the last batch's loss, the epoch's sum of batch losses} (FP64)
+    tsvd::DevMem epoch_users;  // the users of a training epoch, device copy
     tsvd::DevMem tc_err;       // set by the tensor-core GEMM when an MMA wait ran out
     tsvd::DevMem ws;           // split-K partial tiles of the weight-gradient GEMMs
     tsvd::DevMem tws;          // transposed copies of MN-major GEMM operands (TMA path)
@@ -952,8 +999,11 @@ void forward(tsvd_encoder* e, int n) {
          P(e, 8).w.as<float>(), e->y.as<float>(), nullptr, e->O, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
 }
 
-// loss and gradients for n users in e->users (targets from the model)
-double backward(tsvd_encoder* e, int n) {
+// Gradients for n users in e->users (targets from the model). The batch's
+// loss goes to e->loss[0] on the device (and is added to the epoch's sum in
+// e->loss[1] with `acc`); with `read` it is also returned (one stream
+// synchronisation), else 0.
+double backward(tsvd_encoder* e, int n, bool read, bool acc) {
     using namespace tsvd;
     const DeviceState& s = e->model->d;
     cudaStream_t st = e->stream;
@@ -968,7 +1018,7 @@ double backward(tsvd_encoder* e, int n) {
     // layer 3
     gemm(st, e->tc_err.as<unsigned>(), e->h2b.as<__nv_bfloat16>(), 1, kHid, e->dyb.as<__nv_bfloat16>(), 1, Op, kHid, O, n, nullptr,
          P(e, 7).g.as<float>(), nullptr, O, 0, 8, e->ws.as<float>(), e->tws.as<__nv_bfloat16>(), e->tws_elems);
-    k_colsum_f<<<(O + 127) / 128, 128, 0, st>>>(e->dy.as<float>(), n, O, P(e, 8).g.as<float>());
+    colsum<float>(st, e->dy.as<float>(), n, O, e->ws.as<float>(), P(e, 8).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dyb.as<__nv_bfloat16>(), 0, Op, P(e, 7).wb.as<__nv_bfloat16>(), 0, Op, n, kHid, O, nullptr,
          e->dh2.as<float>(), nullptr, kHid, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh2.as<float>(), e->z2.as<float>(), n * kHid,
@@ -976,7 +1026,7 @@ double backward(tsvd_encoder* e, int n) {
     // layer 2
     gemm(st, e->tc_err.as<unsigned>(), e->h1b.as<__nv_bfloat16>(), 1, kHid, e->dz2b.as<__nv_bfloat16>(), 1, kHid, kHid, kHid, n, nullptr,
          P(e, 5).g.as<float>(), nullptr, kHid, 0, 4, e->ws.as<float>(), e->tws.as<__nv_bfloat16>(), e->tws_elems);
-    k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz2b.as<__nv_bfloat16>(), n, kHid, P(e, 6).g.as<float>());
+    colsum<__nv_bfloat16>(st, e->dz2b.as<__nv_bfloat16>(), n, kHid, e->ws.as<float>(), P(e, 6).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dz2b.as<__nv_bfloat16>(), 0, kHid, P(e, 5).wb.as<__nv_bfloat16>(), 0, kHid, n, kHid, kHid, nullptr,
          e->dh1.as<float>(), nullptr, kHid, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     k_gelu_bwd<<<grid_for((size_t)n * kHid), 256, 0, st>>>(e->dh1.as<float>(), e->z1.as<float>(), n * kHid,
@@ -984,7 +1034,7 @@ double backward(tsvd_encoder* e, int n) {
     // layer 1
     gemm(st, e->tc_err.as<unsigned>(), e->h0b.as<__nv_bfloat16>(), 1, kEmb, e->dz1b.as<__nv_bfloat16>(), 1, kHid, kEmb, kHid, n, nullptr,
          P(e, 3).g.as<float>(), nullptr, kHid, 0, 16, e->ws.as<float>(), e->tws.as<__nv_bfloat16>(), e->tws_elems);
-    k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(e->dz1b.as<__nv_bfloat16>(), n, kHid, P(e, 4).g.as<float>());
+    colsum<__nv_bfloat16>(st, e->dz1b.as<__nv_bfloat16>(), n, kHid, e->ws.as<float>(), P(e, 4).g.as<float>());
     gemm(st, e->tc_err.as<unsigned>(), e->dz1b.as<__nv_bfloat16>(), 0, kHid, P(e, 3).wb.as<__nv_bfloat16>(), 0, kHid, n, kEmb, kHid, nullptr,
          e->dh0.as<float>(), nullptr, kEmb, 0, 1, nullptr, e->tws.as<__nv_bfloat16>(), e->tws_elems);
     // embeddings
@@ -994,12 +1044,13 @@ double backward(tsvd_encoder* e, int n) {
     k_hist_grad<<<5 + s.T, kEmb, 0, st>>>(e->hist.as<float>(), 5 + s.T, e->dh0.as<float>(), e->inv_n.as<float>(), n,
                                           P(e, 1).g.as<float>(), P(e, 2).g.as<float>());
     TSVD_CUDA(cudaGetLastError());
-    std::vector<double> part(nb);
-    TSVD_CUDA(cudaMemcpyAsync(part.data(), e->part.p, nb * 8, cudaMemcpyDeviceToHost, st));
+    k_loss<<<1, 32, 0, st>>>(e->part.as<double>(), nb, (double)n * O, e->loss.as<double>(), acc ? 1 : 0);
+    TSVD_CUDA(cudaGetLastError());
+    if (!read) return 0.0;
+    double l = 0.0;
+    TSVD_CUDA(cudaMemcpyAsync(&l, e->loss.p, 8, cudaMemcpyDeviceToHost, st));
     TSVD_CUDA(cudaStreamSynchronize(st));
-    double sse = 0.0;
-    for (double v : part) sse += v;
-    return sse / ((double)n * O);
+    return l;
 }
 
 void adamw_step(tsvd_encoder* e) {
@@ -1151,6 +1202,8 @@ int tsvd_encoder_create(const tsvd_model* m, const int8_t* train_raw, const uint
         e->hist.alloc((size_t)B * (5 + s.T) * 4);
         e->inv_n.alloc((size_t)B * 4);
         e->tc_err.alloc(4);
+        e->loss.alloc(16);
+        TSVD_CUDA(cudaMemset(e->loss.p, 0, 16));
         // split-K slices: dW1 16 x 128 x 512, dW2 4 x 512 x 512, dW3 8 x 512 x O
         e->ws.alloc(std::max(std::max((size_t)16 * kEmb * kHid, (size_t)4 * kHid * kHid), (size_t)8 * kHid * O) * 4);
         // two transposed operands of at most 512 rows x max(batch, 512) columns
@@ -1184,21 +1237,28 @@ int tsvd_encoder_train_epoch(tsvd_encoder* e, const uint32_t* users, uint64_t n,
     return eguard(e, [&] {
         if (batch == 0 || batch > (uint32_t)tsvd::kMaxBatch) throw Error(TSVD_ERR_INVALID, "batch must be 1..4096");
         TSVD_CUDA(cudaSetDevice(e->model->device));
-        double tot = 0.0;
+        for (uint64_t k = 0; k < n; ++k)
+            if (users[k] >= e->model->d.n_users) throw Error(TSVD_ERR_INVALID, "user out of range");
+        // the batches' users go up once; the batch losses are summed on the
+        // device, so the epoch runs without a host round trip per batch
+        if (e->epoch_users.bytes < n * 4) e->epoch_users.alloc(n * 4);
+        TSVD_CUDA(cudaMemcpyAsync(e->epoch_users.p, users, n * 4, cudaMemcpyHostToDevice, e->stream));
+        TSVD_CUDA(cudaMemsetAsync(e->loss.p, 0, 16, e->stream));
         uint64_t nb = 0;
         for (uint64_t a = 0; a < n; a += batch) {
             const int b = (int)std::min<uint64_t>(batch, n - a);
-            for (int k = 0; k < b; ++k)
-                if (users[a + k] >= e->model->d.n_users) throw Error(TSVD_ERR_INVALID, "user out of range");
-            set_users(e, users + a, b);
+            TSVD_CUDA(cudaMemcpyAsync(e->users.p, e->epoch_users.as<uint32_t>() + a, (size_t)b * 4,
+                                      cudaMemcpyDeviceToDevice, e->stream));
             forward(e, b);
-            tot += backward(e, b);
+            backward(e, b, false, true);
             adamw_step(e);
             nb++;
         }
+        double sums[2] = {0.0, 0.0};
+        TSVD_CUDA(cudaMemcpyAsync(sums, e->loss.p, 16, cudaMemcpyDeviceToHost, e->stream));
         TSVD_CUDA(cudaStreamSynchronize(e->stream));
         check_tc(e);
-        e->last_loss = nb ? tot / nb : 0.0;
+        e->last_loss = nb ? sums[1] / nb : 0.0;
         if (mean_loss) *mean_loss = e->last_loss;
     });
 }
@@ -1213,7 +1273,7 @@ int tsvd_encoder_loss_grad(tsvd_encoder* e, const uint32_t* users, uint32_t n, d
         TSVD_CUDA(cudaSetDevice(e->model->device));
         set_users(e, users, (int)n);
         forward(e, (int)n);
-        const double l = backward(e, (int)n);
+        const double l = backward(e, (int)n, true, false);
         check_tc(e);
         if (loss) *loss = l;
     });

@@ -83,6 +83,16 @@ __global__ void k_iota(uint32_t* __restrict__ v, uint64_t n) {
         v[k] = (uint32_t)k;
 }
 
+// off[j] = the first position t of the sorted keys with key >= j (j = 0..I),
+// so item j's entries are off[j] .. off[j+1]-1; each j is written once.
+__global__ void k_item_offsets(const uint32_t* __restrict__ sorted, uint64_t R, uint32_t I, uint64_t* __restrict__ off) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= R; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = t == 0 ? 0u : sorted[t - 1] + 1u;
+        const uint32_t b = t == R ? I : sorted[t];
+        for (uint32_t j = a; j <= b; ++j) off[j] = t;
+    }
+}
+
 __global__ void k_fill(float* __restrict__ v, uint64_t n, float x) {
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
         v[k] = x;
@@ -154,6 +164,20 @@ int bits_for(uint64_t maxv) {
 
 }  // namespace
 
+// 0 .. n-1 ordered by count, largest first, ties in index order: a stable
+// counting sort, the same order as a stable sort by descending count.
+template <class C>
+std::vector<uint32_t> heaviest_first(const C* cnt, uint32_t n) {
+    uint64_t mx = 0;
+    for (uint32_t i = 0; i < n; ++i) mx = std::max<uint64_t>(mx, (uint64_t)cnt[i]);
+    std::vector<uint32_t> start(mx + 2, 0u);
+    for (uint32_t i = 0; i < n; ++i) start[mx - (uint64_t)cnt[i] + 1]++;
+    for (uint64_t b = 1; b < start.size(); ++b) start[b] += start[b - 1];
+    std::vector<uint32_t> out(n);
+    for (uint32_t i = 0; i < n; ++i) out[start[mx - (uint64_t)cnt[i]]++] = i;
+    return out;
+}
+
 void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_view& pr) {
     const tsvd_config& c = m->cfg;
     cudaStream_t st = m->stream;
@@ -208,6 +232,17 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
 
     const uint32_t U = (uint32_t)tr.n_users, I = (uint32_t)tr.n_items;
     const uint64_t R = tr.n_ratings, P = pr.n_ratings;
+    // The raw columns go up first, so that the copies (asynchronous from pinned
+    // buffers) overlap the host-side checks and sums below; nothing on the
+    // device reads them before those checks have passed.
+    DevMem d_tu, d_ti, d_td, d_tres, d_pu, d_pi, d_pd, tmp;
+    upload(d_tu, tr.user_idxs, R, st);
+    upload(d_ti, tr.item_idxs, R, st);
+    upload(d_td, tr.dates, R, st);
+    if (!c.has_ordinal_head) upload(d_tres, tr.residuals, R, st);
+    upload(d_pu, pr.user_idxs, P, st);
+    upload(d_pi, pr.item_idxs, P, st);
+    upload(d_pd, pr.dates, P, st);
     // calc_user_offsets (src/lib.rs:470-483): user-sorted, offsets from user_cnts.
     std::vector<uint64_t> uoff(U + 1, 0);
     for (uint32_t u = 0; u < U; ++u) {
@@ -289,11 +324,7 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
     s.gbias = (float)(rsum / (double)R);
     m->h_user_cnt.assign(tr.user_cnts, tr.user_cnts + U);
 
-    // ---- upload raw columns -------------------------------------------------
-    DevMem d_tu, d_ti, d_td, d_tres, d_pu, d_pi, d_pd, tmp;
-    upload(d_tu, tr.user_idxs, R, st);
-    upload(d_ti, tr.item_idxs, R, st);
-    upload(d_td, tr.dates, R, st);
+    // ---- upload raw columns (the rest; see above) ------------------------------
     if (c.has_ordinal_head) {
         // with the head the error comes from the raw rating, not the residual
         // (src/tx.rs:965-969): the records carry the raw rating instead
@@ -301,12 +332,7 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         for (uint64_t t = 0; t < R; ++t) rawf[t] = (float)tr.raw_ratings[t];
         upload(d_tres, rawf.data(), R, st);
         TSVD_CUDA(cudaStreamSynchronize(st));
-    } else {
-        upload(d_tres, tr.residuals, R, st);
     }
-    upload(d_pu, pr.user_idxs, P, st);
-    upload(d_pi, pr.item_idxs, P, st);
-    upload(d_pd, pr.dates, P, st);
     upload(m->m_user_off, uoff.data(), U + 1, st);
     upload(m->m_tu_mean, tum.data(), U, st);
     s.raw = nullptr;
@@ -441,29 +467,22 @@ void setup_model(tsvd_model* m, const tsvd_dataset_view& tr, const tsvd_dataset_
         k_item_records<<<kGrid, kBlock, 0, st>>>(m->m_rec.as<Rec>(), d_tu.as<int32_t>(), idx_sorted.as<uint32_t>(), R,
                                                  m->m_irec.as<Rec>());
         TSVD_CUDA(cudaGetLastError());
+        // item offsets from the sorted item keys, on the device
+        m->m_item_off.alloc((size_t)(I + 1) * 8);
+        k_item_offsets<<<kGrid, kBlock, 0, st>>>(ikey_sorted.as<uint32_t>(), R, I, m->m_item_off.as<uint64_t>());
+        TSVD_CUDA(cudaGetLastError());
         std::vector<uint64_t> ioff(I + 1, 0);
-        std::vector<uint32_t> icnt(I, 0);
-#pragma omp parallel
-        {
-            std::vector<uint32_t> mine(I, 0);
-#pragma omp for schedule(static) nowait
-            for (int64_t t = 0; t < (int64_t)R; ++t) mine[tr.item_idxs[t]]++;
-#pragma omp critical
-            for (uint32_t i = 0; i < I; ++i) icnt[i] += mine[i];
-        }
-        for (uint32_t i = 0; i < I; ++i) ioff[i + 1] = ioff[i] + icnt[i];
-        upload(m->m_item_off, ioff.data(), I + 1, st);
+        TSVD_CUDA(cudaMemcpyAsync(ioff.data(), m->m_item_off.p, (size_t)(I + 1) * 8, cudaMemcpyDeviceToHost, st));
+        TSVD_CUDA(cudaStreamSynchronize(st));
+        std::vector<uint64_t> icnt(I, 0);
+        for (uint32_t i = 0; i < I; ++i) icnt[i] = ioff[i + 1] - ioff[i];
+        m->h_item_off = ioff;
         s.irec = m->m_irec.as<Rec>();
         s.item_off = m->m_item_off.as<uint64_t>();
         // work lists: heaviest first (longest-processing-time order)
-        std::vector<uint32_t> iw(I);
-        std::iota(iw.begin(), iw.end(), 0u);
-        std::stable_sort(iw.begin(), iw.end(), [&](uint32_t a, uint32_t b) { return icnt[a] > icnt[b]; });
+        const std::vector<uint32_t> iw = heaviest_first(icnt.data(), I);
         upload(m->m_item_work, iw.data(), I, st);
-        std::vector<uint32_t> uw(U);
-        std::iota(uw.begin(), uw.end(), 0u);
-        std::stable_sort(uw.begin(), uw.end(),
-                         [&](uint32_t a, uint32_t b) { return tr.user_cnts[a] > tr.user_cnts[b]; });
+        const std::vector<uint32_t> uw = heaviest_first(tr.user_cnts, U);
         upload(m->m_user_work, uw.data(), U, st);
         s.item_work = m->m_item_work.as<uint32_t>();
         s.n_item_work = I;

@@ -57,15 +57,30 @@ bool find_param(const tsvd_model* m, const std::string& n, ParamRef& r) {
 
 const char* kSubscoreNames[3] = {"bias", "mf", "nsvd1"};
 
-template <class T>
-struct DevCopy {
-    tsvd::DevMem mem;
-    const T* ptr = nullptr;
-    void from(const T* h, uint64_t n, cudaStream_t st) {
-        if (!h) return;
-        mem.alloc(n * sizeof(T));
-        TSVD_CUDA(cudaMemcpyAsync(mem.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
-        ptr = mem.as<T>();
+// Device copies of a call's host row columns in the model's staging buffer:
+// reserve() sizes it for the call, put() copies one column (256-byte aligned
+// slots), out() hands out an uninitialised slot.
+struct RowStage {
+    char* base = nullptr;
+    size_t off = 0;
+    static size_t slot(size_t bytes) { return (bytes + 255) / 256 * 256; }
+    RowStage(const tsvd_model* m, size_t bytes) {
+        if (m->m_rows.bytes < bytes) m->m_rows.alloc(bytes);
+        base = m->m_rows.as<char>();
+    }
+    template <class T>
+    const T* put(const T* h, uint64_t n, cudaStream_t st) {
+        if (!h) return nullptr;
+        T* d = reinterpret_cast<T*>(base + off);
+        TSVD_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+        off += slot(n * sizeof(T));
+        return d;
+    }
+    template <class T>
+    T* out(uint64_t n) {
+        T* d = reinterpret_cast<T*>(base + off);
+        off += slot(n * sizeof(T));
+        return d;
     }
 };
 
@@ -194,6 +209,13 @@ int tsvd_predict_batch_device(const tsvd_model* m, const int32_t* u, const int32
 }
 
 static void check_rows(const tsvd_model* m, const int32_t* u, const int32_t* i, uint64_t n) {
+    // in parallel; a failure reruns the check in row order for the first bad row
+    const uint32_t U = m->d.n_users, I = m->d.n_items;
+    bool ok = true;
+#pragma omp parallel for schedule(static) reduction(&& : ok) if (n > 65536)
+    for (int64_t k = 0; k < (int64_t)n; ++k)
+        ok = ok && u[k] >= 0 && (uint32_t)u[k] < U && i[k] >= 0 && (uint32_t)i[k] < I;
+    if (ok) return;
     for (uint64_t k = 0; k < n; ++k)
         if (u[k] < 0 || (uint32_t)u[k] >= m->d.n_users || i[k] < 0 || (uint32_t)i[k] >= m->d.n_items)
             throw Error(TSVD_ERR_INVALID, "row " + std::to_string(k) + ": user or item index out of range");
@@ -209,18 +231,16 @@ static int predict_host(const tsvd_model* m, const int32_t* u, const int32_t* i,
         check_rows(m, u, i, n);
         use_device(m);
         cudaStream_t st = m->stream;
-        DevCopy<int32_t> du, di;
-        DevCopy<int16_t> dd;
-        DevCopy<float> doff;
-        du.from(u, n, st);
-        di.from(i, n, st);
-        dd.from(day, n, st);
-        doff.from(offset, n, st);
-        tsvd::DevMem dout;
         const uint64_t cols = subscores ? 3 : 1;
-        dout.alloc(n * cols * sizeof(float));
-        tsvd::predict_device(m, du.ptr, di.ptr, dd.ptr, doff.ptr, n, dout.as<float>(), subscores);
-        TSVD_CUDA(cudaMemcpyAsync(out, dout.p, n * cols * sizeof(float), cudaMemcpyDeviceToHost, st));
+        RowStage rs(m, 2 * RowStage::slot(n * 4) + RowStage::slot(n * 2) + RowStage::slot(n * 4) +
+                           RowStage::slot(n * cols * 4));
+        const int32_t* du = rs.put(u, n, st);
+        const int32_t* di = rs.put(i, n, st);
+        const int16_t* dd = rs.put(day, n, st);
+        const float* doff = rs.put(offset, n, st);
+        float* dout = rs.out<float>(n * cols);
+        tsvd::predict_device(m, du, di, dd, doff, n, dout, subscores);
+        TSVD_CUDA(cudaMemcpyAsync(out, dout, n * cols * sizeof(float), cudaMemcpyDeviceToHost, st));
         TSVD_CUDA(cudaStreamSynchronize(st));
     });
 }
@@ -263,17 +283,14 @@ int tsvd_calc_rmse(const tsvd_model* m, const tsvd_dataset_view* ds, double* out
         check_rows(m, ds->user_idxs, ds->item_idxs, n);
         use_device(m);
         cudaStream_t st = m->stream;
-        DevCopy<int32_t> du, di;
-        DevCopy<int16_t> dd;
-        DevCopy<float> dr;
-        DevCopy<int8_t> dt;
-        du.from(ds->user_idxs, n, st);
-        di.from(ds->item_idxs, n, st);
-        dd.from(ds->dates, n, st);
-        dr.from(ds->residuals, n, st);
-        dt.from(ds->is_test, n, st);
+        RowStage rs(m, 3 * RowStage::slot(n * 4) + RowStage::slot(n * 2) + RowStage::slot(n));
+        const int32_t* du = rs.put(ds->user_idxs, n, st);
+        const int32_t* di = rs.put(ds->item_idxs, n, st);
+        const int16_t* dd = rs.put(ds->dates, n, st);
+        const float* dr = rs.put(ds->residuals, n, st);
+        const int8_t* dt = rs.put(ds->is_test, n, st);
         double sse = 0.0, cnt = 0.0;
-        tsvd::sse_device(m, du.ptr, di.ptr, dd.ptr, dr.ptr, dt.ptr, n, &sse, &cnt);
+        tsvd::sse_device(m, du, di, dd, dr, dt, n, &sse, &cnt);
         *out = std::sqrt(sse / cnt);
     });
 }

@@ -176,7 +176,9 @@ struct tsvd_model {
     tsvd::DevMem m_perm;          // [U] epoch order upload buffer
     tsvd::DevMem m_shard_work;    // a sharded run's block work list (users or items)
     tsvd::DevMem m_scratch;       // predict / rmse scratch
-    size_t scratch_rows = 0;
+    // host-buffer entry points (predict, calc_rmse): their rows' device copies,
+    // one buffer grown as needed (the model's mutex serialises the calls)
+    mutable tsvd::DevMem m_rows;
 
     std::vector<uint32_t> h_user_cnt;  // train counts (host copy)
     std::vector<uint64_t> h_item_off;  // by-item offsets (host copy, made on first use)

@@ -217,9 +217,10 @@ void sse_device(const tsvd_model* mc, const int32_t* u, const int32_t* i, const 
     ProfScope ps(m, "sse");
     PredParams pp{m->cfg.beta, m->cfg.low_memory, m->cfg.has_ordinal_head};
     const int vpl = (int)std::min<uint32_t>(m->d.Fs / 32, 8);
-    DevMem part;
-    part.alloc((2 * kSseBlocks + 2) * sizeof(double));
-    double* psse = part.as<double>();
+    // the block partials in the model's scratch (allocated on the first call)
+    const size_t need = (2 * kSseBlocks + 2) * sizeof(double);
+    if (m->m_scratch.bytes < need) m->m_scratch.alloc(need);
+    double* psse = m->m_scratch.as<double>();
     double* pcnt = psse + kSseBlocks;
     double* fin = pcnt + kSseBlocks;
     TSVD_DISPATCH(vpl, (k_sse<V><<<kSseBlocks, kThreads, 0, m->stream>>>(m->d, pp, u, i, day, target, is_test, n, psse,

@@ -379,11 +379,16 @@ __device__ __forceinline__ void rebuild_user(const DeviceState& s, const __nv_bf
 #pragma unroll
         for (int v = 0; v < VPL; ++v) su[v] = 0.0f;
         float sub = 0.0f;
+        // the item of entry q of N(u): training ratings first, then pr items
+        auto item_at = [&](uint64_t q) -> uint32_t {
+            return q < ntr ? rec_id(__ldg(&s.rec[a + q].key)) : __ldg(s.pr_item + pa + (q - ntr));
+        };
+        // each chunk's 32 items are loaded one chunk ahead (one per lane)
+        uint32_t nxt = (uint64_t)lane < n ? item_at(lane) : 0u;
         for (uint64_t base = 0; base < n; base += 32) {
             const uint32_t cnt = (uint32_t)(n - base < 32 ? n - base : 32);
-            const uint64_t q = base + lane;
-            uint32_t mine = 0;
-            if (lane < (int)cnt) mine = q < ntr ? rec_id(__ldg(&s.rec[a + q].key)) : __ldg(s.pr_item + pa + (q - ntr));
+            const uint32_t mine = nxt;
+            if (base + 32 + lane < n) nxt = item_at(base + 32 + lane);
             for (uint32_t j = 0; j < cnt; j += B) {
                 float y[B][VPL], yb[B];
 #pragma unroll

@@ -162,17 +162,18 @@ void enqueue_epoch(tsvd_group* g) {
     tsvd::launch_rebuild_batched(st, g->d_states.as<tsvd::DeviceState>(), n, U);
 }
 
-// Every variant's stratified epoch on its own stream, forked from and joined
-// to the group's stream.
+// Every variant's stratified epoch on its own stream: all forked from one
+// point of the group's stream, all joined back after every variant's epoch is
+// enqueued, so the variants' kernels run concurrently.
 void enqueue_strat_epoch(tsvd_group* g, uint64_t epoch) {
+    TSVD_CUDA(cudaEventRecord(g->fork[0], g->stream));
     for (size_t k = 0; k < g->models.size(); ++k) {
         tsvd_model* m = g->models[k];
-        TSVD_CUDA(cudaEventRecord(g->fork[k], g->stream));
-        TSVD_CUDA(cudaStreamWaitEvent(m->stream, g->fork[k], 0));
+        TSVD_CUDA(cudaStreamWaitEvent(m->stream, g->fork[0], 0));
         tsvd::run_epoch(m, epoch);
         TSVD_CUDA(cudaEventRecord(g->join[k], m->stream));
-        TSVD_CUDA(cudaStreamWaitEvent(g->stream, g->join[k], 0));
     }
+    for (size_t k = 0; k < g->models.size(); ++k) TSVD_CUDA(cudaStreamWaitEvent(g->stream, g->join[k], 0));
 }
 
 void drop_graph(tsvd_group* g) {

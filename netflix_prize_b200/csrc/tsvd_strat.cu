@@ -129,8 +129,11 @@ __device__ __forceinline__ void dyd_add(unsigned long long* row, int lane, const
 // sqrt(day count) goes to every item of the run as a yfeat_day delta
 // (:614-622).
 // ---------------------------------------------------------------------------
+// Three blocks per SM without the per-day terms: the kernel is issue-bound, and
+// the extra resident warps outweigh a few spilled registers (full shape, f =
+// 256: 26.2 -> 24.2 ms per user stratum).
 template <int VPL, bool BF, bool DAY>
-__global__ void __launch_bounds__(kThreads) k_user_strat(DeviceState s, EpochParams p, Bf16Copies bf,
+__global__ void __launch_bounds__(kThreads, DAY ? 2 : 3) k_user_strat(DeviceState s, EpochParams p, Bf16Copies bf,
                                                          const uint32_t* __restrict__ order, uint32_t n_work) {
     // FP32 with low_memory: the rating's item rows are read as their sum qe0
     constexpr bool QE = !BF && !DAY;

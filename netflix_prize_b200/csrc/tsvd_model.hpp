@@ -181,6 +181,7 @@ struct tsvd_model {
     mutable tsvd::DevMem m_rows;
 
     std::vector<uint32_t> h_user_cnt;  // train counts (host copy)
+    uint32_t h_max_user_cnt = 0;       // the largest of them (made on first use)
     std::vector<uint64_t> h_item_off;  // by-item offsets (host copy, made on first use)
     std::vector<uint64_t> h_ud_start;  // (user, day) offsets per user (host copy, made on first use)
     std::map<uint64_t, std::vector<uint32_t>> injected_order;

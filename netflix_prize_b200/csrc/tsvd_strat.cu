@@ -129,11 +129,12 @@ __device__ __forceinline__ void dyd_add(unsigned long long* row, int lane, const
 // sqrt(day count) goes to every item of the run as a yfeat_day delta
 // (:614-622).
 // ---------------------------------------------------------------------------
-// Three blocks per SM without the per-day terms: the kernel is issue-bound, and
-// the extra resident warps outweigh a few spilled registers (full shape, f =
-// 256: 26.2 -> 24.2 ms per user stratum).
-template <int VPL, bool BF, bool DAY>
-__global__ void __launch_bounds__(kThreads, DAY ? 2 : 3) k_user_strat(DeviceState s, EpochParams p, Bf16Copies bf,
+// MINB blocks per SM. Three (a few registers spilled) pay off where the pass
+// is bound by its total work rather than by its longest user chains, which
+// every extra resident warp slows: 26.2 -> 24.2 ms at the full shape, f = 256,
+// but 10.0 -> 12.2 ms on 120,000 users with the same most active users.
+template <int VPL, bool BF, bool DAY, int MINB = 2>
+__global__ void __launch_bounds__(kThreads, MINB) k_user_strat(DeviceState s, EpochParams p, Bf16Copies bf,
                                                          const uint32_t* __restrict__ order, uint32_t n_work) {
     // FP32 with low_memory: the rating's item rows are read as their sum qe0
     constexpr bool QE = !BF && !DAY;
@@ -1507,6 +1508,20 @@ void strat_launch_wide(tsvd_model* m, const EpochParams& p) {
     }
 }
 
+// Whether the user stratum of the whole user set is bound by its total work
+// rather than by its longest user chains: the ratings per warp at three blocks
+// per SM at least the most active user's count (1.66x at the full Netflix
+// shape, 0.41x on 120,000 users).
+bool user_stratum_work_bound(tsvd_model* m) {
+    if (m->h_max_user_cnt == 0)
+        for (uint32_t c : m->h_user_cnt) m->h_max_user_cnt = std::max(m->h_max_user_cnt, c);
+    int dev = 0, sms = 0;
+    TSVD_CUDA(cudaGetDevice(&dev));
+    TSVD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const double warps = (double)sms * 3 * kWarps;
+    return (double)m->d.n_train / warps >= (double)std::max<uint32_t>(m->h_max_user_cnt, 1u);
+}
+
 void make_qe0(tsvd_model* m) {
     const DeviceState& s = m->d;
     if (!s.qe0) return;
@@ -1538,8 +1553,13 @@ void strat_launch(tsvd_model* m, const EpochParams& p, const Bf16Copies& bf) {
     if (!BF && !DAY) make_qe0(m);
     {
         ProfScope ps(m, "user_pass_stratified");
-        unsigned g = persistent_grid(k_user_strat<VPL, BF, DAY>, 0);
-        k_user_strat<VPL, BF, DAY><<<g, kThreads, 0, m->stream>>>(s, p, bf, s.user_work, s.n_users);
+        if (!DAY && user_stratum_work_bound(m)) {
+            unsigned g = persistent_grid(k_user_strat<VPL, BF, DAY, 3>, 0);
+            k_user_strat<VPL, BF, DAY, 3><<<g, kThreads, 0, m->stream>>>(s, p, bf, s.user_work, s.n_users);
+        } else {
+            unsigned g = persistent_grid(k_user_strat<VPL, BF, DAY>, 0);
+            k_user_strat<VPL, BF, DAY><<<g, kThreads, 0, m->stream>>>(s, p, bf, s.user_work, s.n_users);
+        }
         TSVD_CUDA(cudaGetLastError());
         m->launches++;
     }

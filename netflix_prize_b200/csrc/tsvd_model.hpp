@@ -174,6 +174,9 @@ struct tsvd_model {
     tsvd::DevMem m_bf_ifeat, m_bf_qf0, m_bf_yfeat, m_bf_pyc, m_bf_ufeat2;
     tsvd::DevMem m_chunk_lo, m_item_chunk0, m_chunk_part, m_chunk_epart;
     tsvd::DevMem m_perm;          // [U] epoch order upload buffer
+    // NSVD1 delta-sum passes: per chunk, the positions where the passes' user
+    // blocks start ([n_chunks, passes + 1]), for the block bounds last used
+    tsvd::DevMem m_chunk_split, m_split_bounds;
     tsvd::DevMem m_shard_work;    // a sharded run's block work list (users or items)
     tsvd::DevMem m_scratch;       // predict / rmse scratch
     // host-buffer entry points (predict, calc_rmse): their rows' device copies,
@@ -182,6 +185,7 @@ struct tsvd_model {
 
     std::vector<uint32_t> h_user_cnt;  // train counts (host copy)
     uint32_t h_max_user_cnt = 0;       // the largest of them (made on first use)
+    std::vector<uint32_t> h_split_bounds;  // user-block bounds of the delta-sum passes (m_chunk_split)
     std::vector<uint64_t> h_item_off;  // by-item offsets (host copy, made on first use)
     std::vector<uint64_t> h_ud_start;  // (user, day) offsets per user (host copy, made on first use)
     std::map<uint64_t, std::vector<uint32_t>> injected_order;

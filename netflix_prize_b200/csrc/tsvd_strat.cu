@@ -338,8 +338,11 @@ __global__ void __launch_bounds__(kThreads, MINB) k_user_strat(DeviceState s, Ep
 // chunks without entries in the block are left alone: passes over user blocks
 // whose g_user rows fit in L2 gather from L2 instead of HBM.
 template <int VPL>
+// split (optional): per chunk, the first entry of each pass's user block
+// (split[c * (passes + 1) + k]); without it the block's range is searched.
 __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t u_lo, uint32_t u_hi,
-                                                        int accumulate) {
+                                                        int accumulate, const uint64_t* __restrict__ split,
+                                                        uint32_t passes, uint32_t pass) {
     const int lane = threadIdx.x & 31;
     const uint32_t Fs = s.Fs;
     constexpr int B = 8;  // rows in flight per warp
@@ -351,7 +354,11 @@ __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t 
         uint64_t a = s.chunk_lo[c];
         uint64_t b = s.chunk_lo[c + 1];
         if (b - a > kChunkUsers) b = a + kChunkUsers;
-        if (u_lo != 0 || u_hi != 0xffffffffu) {
+        if (split) {
+            a = split[(size_t)c * (passes + 1) + pass];
+            b = split[(size_t)c * (passes + 1) + pass + 1];
+            if (accumulate && a == b) continue;
+        } else if (u_lo != 0 || u_hi != 0xffffffffu) {
             // the chunk's entries of users u_lo..u_hi-1 (sorted by user)
             uint64_t lo = a, hi = b;
             while (lo < hi) {
@@ -409,23 +416,74 @@ __global__ void __launch_bounds__(kThreads) k_y_partial(DeviceState s, uint32_t 
     }
 }
 
+// split[c * (nb) + k] = the first entry of chunk c whose user is >= bounds[k]
+// (the chunk's entries are sorted by user).
+__global__ void k_chunk_splits(DeviceState s, const uint32_t* __restrict__ bounds, uint32_t nb,
+                               uint64_t* __restrict__ split) {
+    const uint64_t n = (uint64_t)s.n_chunks * nb;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(e / nb), k = (uint32_t)(e % nb);
+        uint64_t lo = s.chunk_lo[c], hi = s.chunk_lo[c + 1];
+        if (hi - lo > kChunkUsers) hi = lo + kChunkUsers;
+        const uint32_t u = bounds[k];
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (rec_id(__ldg(&s.irec[mid].key)) < u) lo = mid + 1;
+            else hi = mid;
+        }
+        split[e] = lo;
+    }
+}
+
+// The per-chunk split table for the user-block bounds `bounds`, made when the
+// bounds change (outside a stream capture; inside one, a stale table gives
+// null and the passes search instead).
+const uint64_t* chunk_splits(tsvd_model* m, const DeviceState& s, const std::vector<uint32_t>& bounds) {
+    if (bounds != m->h_split_bounds || !m->m_chunk_split.p) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        TSVD_CUDA(cudaStreamIsCapturing(m->stream, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return nullptr;
+        const size_t n = (size_t)s.n_chunks * bounds.size();
+        if (m->m_chunk_split.bytes < n * 8) m->m_chunk_split.alloc(n * 8);
+        if (m->m_split_bounds.bytes < bounds.size() * 4) m->m_split_bounds.alloc(bounds.size() * 4);
+        TSVD_CUDA(cudaMemcpyAsync(m->m_split_bounds.p, bounds.data(), bounds.size() * 4, cudaMemcpyHostToDevice,
+                                  m->stream));
+        const unsigned grid = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+        k_chunk_splits<<<grid, 256, 0, m->stream>>>(s, m->m_split_bounds.as<uint32_t>(), (uint32_t)bounds.size(),
+                                                    m->m_chunk_split.as<uint64_t>());
+        TSVD_CUDA(cudaGetLastError());
+        TSVD_CUDA(cudaStreamSynchronize(m->stream));  // `bounds` is the caller's
+        m->launches++;
+        m->h_split_bounds = bounds;
+    }
+    return m->m_chunk_split.as<uint64_t>();
+}
+
 // The NSVD1 delta sums of users u_lo..u_hi-1 into the chunk partials, in
 // passes over user blocks of at most ~64 MB of g_user rows (L2 holds one).
+// Each chunk's entries of a block come from a split table made once for the
+// blocks' bounds, not from a search in every pass.
 template <int VPL>
 void y_partial_passes(tsvd_model* m, const DeviceState& s, uint32_t u_lo, uint32_t u_hi) {
     const uint64_t row_bytes = (uint64_t)s.Fs * 4;
     const uint32_t per = (uint32_t)std::max<uint64_t>(1, (64ull << 20) / row_bytes);
     const unsigned g = persistent_grid(k_y_partial<VPL>, 0);
     const bool whole = u_lo == 0 && u_hi >= s.n_users;
+    std::vector<uint32_t> bounds;
     for (uint64_t b0 = u_lo; b0 < u_hi || b0 == u_lo; b0 += per) {
-        const uint32_t b1 = (uint32_t)std::min<uint64_t>(u_hi, b0 + per);
+        bounds.push_back((uint32_t)b0);
+        if (std::min<uint64_t>(u_hi, b0 + per) >= u_hi) break;
+    }
+    bounds.push_back(u_hi);
+    const uint32_t passes = (uint32_t)bounds.size() - 1;
+    const bool one = whole && passes == 1;  // a single pass over every user
+    const uint64_t* split = one ? nullptr : chunk_splits(m, s, bounds);
+    for (uint32_t k = 0; k < passes; ++k) {
         TSVD_CUDA(cudaMemsetAsync(s.counters + 1, 0, 4, m->stream));
-        const bool one = whole && b1 >= u_hi && b0 == u_lo;  // a single pass over every user
-        k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, one ? 0u : (uint32_t)b0, one ? 0xffffffffu : b1,
-                                                        b0 == u_lo ? 0 : 1);
+        k_y_partial<VPL><<<g, kThreads, 0, m->stream>>>(s, one ? 0u : bounds[k], one ? 0xffffffffu : bounds[k + 1],
+                                                        k == 0 ? 0 : 1, split, passes, k);
         TSVD_CUDA(cudaGetLastError());
         m->launches++;
-        if (b1 >= u_hi) break;
     }
 }
 
